@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""Benchmark: time to k eigenpairs at relative residual 1e-10 on one B200 (FP64 and mixed
+precision) through trl's unchanged BlockLanczos driver on the CUDA backend, with SpMM and
+block-kernel GB/s measured live during the timed solves.
+
+Workload (default): the 96^3 3-D 7-point anisotropic Laplacian, axis coefficients
+(1, 10, 100) (n = 884,736, nnz = 6,137,856, FP64 CSR), block size 8, the 32 largest
+eigenpairs, basis 48 blocks (ncv = 384), thick restart, tolerance 1e-10; seeded synthetic
+start block. A "step" is one complete solve (Ritz vectors and true residuals included) from
+the same start block with the operator already resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl trl|reference]
+
+--impl reference times the reference's own OpenMP implementation (the oracle built from the
+reference sources) on the host cores: each step is a bounded sample (the first two restart
+cycles), projected to a full solve with the reference's restart count for this workload.
+With --gpus N > 1 (torchrun), each rank solves the same workload on its own GPU (the
+eigensolver does not shard: replicas only); timings are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to k eigenpairs at rel. residual 1e-10: mixed vs FP64 on B200; SpMM GB/s"
+CFG = dict(grid=96, coef=(1.0, 10.0, 100.0), bs=8, nev=32, ncv=384, tol=1e-10, seed=42)
+WORKLOAD = "anisotropic3d-96^3 (1,10,100) n=884736 nnz=6137856 bs=8 nev=32 ncv=384 tol=1e-10"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d.get("bf16_tflops"), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args, world, rank):
+    """The reference's OpenMP path on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from trl_b200 import problems as P
+
+    if not O.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference checkout at build time)"}))
+        return
+    ref = load_reference_counts()
+    A = P.anisotropic3d(CFG["grid"], coef=CFG["coef"])
+    X0 = P.initial_block(A.n, CFG["bs"], seed=CFG["seed"])
+    per_restart = []
+    for i in range(args.warmup + args.steps):
+        s = cpu_restart_sample(O, A, X0)
+        if i >= args.warmup:
+            per_restart.append(s["per_restart"])
+    t_restart = statistics.mean(per_restart)
+    value = t_restart * ref["restarts"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "host OpenMP", "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": O.num_threads(), "kind": "reference",
+                         "sample": f"first 2 restart cycles of the reference BlockLanczos (ModifiedGS, CholQR) per step; steady-state restart "
+                                   f"{t_restart:.3f} s x {ref['restarts']} restarts (the reference's count for this workload, "
+                                   f"tests/golden/cfg2_reference.json)"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def load_reference_counts() -> dict:
+    path = os.path.join(ROOT, "tests", "golden", "cfg2_reference.json")
+    with open(path) as f:
+        return json.load(f)
+
+
+def cpu_restart_sample(O, A, X0) -> dict:
+    """Times 1 and 2 restart cycles of the oracle; the difference is one steady-state cycle."""
+    r1 = O.solve_csr(A, CFG["bs"], CFG["nev"], CFG["ncv"], X0, tol=CFG["tol"], max_restarts=1)
+    r2 = O.solve_csr(A, CFG["bs"], CFG["nev"], CFG["ncv"], X0, tol=CFG["tol"], max_restarts=2)
+    return {"first": r1["seconds"], "two": r2["seconds"], "per_restart": max(r2["seconds"] - r1["seconds"], 1e-9)}
+
+
+def trl_arm(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    from trl_b200 import native
+    from trl_b200 import problems as P
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    bs, nev, ncv, tol = CFG["bs"], CFG["nev"], CFG["ncv"], CFG["tol"]
+    A = P.anisotropic3d(CFG["grid"], coef=CFG["coef"])
+    exact = P.anisotropic3d_eigenvalues(CFG["grid"], coef=CFG["coef"], k=nev)
+    X0 = P.initial_block(A.n, bs, seed=CFG["seed"])
+    h = native.Handle(local)
+    A64 = native.DeviceCSRTensors.from_host(A, torch.float64)
+    A32 = native.DeviceCSRTensors.from_host(A, torch.float32)
+    X0d = torch.from_numpy(X0).cuda()
+    evecs = torch.empty((A.n, nev), dtype=torch.float64, device="cuda")
+    common = dict(bs=bs, nev=nev, ncv=ncv, tol=tol, max_restarts=2000, refine_max_restarts=2000, fp32_tol=args.fp32_tol, want_vectors=1)
+
+    def solve(mode):
+        return native.solve_csr_device(h, A64, A32, X0d, evecs=evecs, mode=mode, **common)
+
+    def timed(mode, steps, profile=False):
+        barrier()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if profile:
+            h.profile(True)
+        launches0 = h.launches()
+        outs = []
+        start.record()
+        for _ in range(steps):
+            outs.append(solve(mode))
+        end.record()
+        torch.cuda.synchronize()
+        prof = h.profile_read() if profile else None
+        if profile:
+            h.profile(False)
+        barrier()
+        ms = start.elapsed_time(end) / steps
+        return max_over_ranks(ms), outs, prof, h.launches() - launches0
+
+    for _ in range(args.warmup):
+        solve(native.TRL_MODE_FP64)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms64, outs64, prof, launches = timed(native.TRL_MODE_FP64, args.steps, profile=True)
+    clk = clocks.stop()
+    o64 = outs64[-1]
+    for _ in range(min(args.warmup, 1)):
+        solve(native.TRL_MODE_MIXED)
+    msmx, outsmx, _, _ = timed(native.TRL_MODE_MIXED, args.steps)
+    omx = outsmx[-1]
+
+    # ---- e2e: host buffers through trl_solve_csr_host, H2D/D2H inside the timed region ----
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    Ah = P.CSRMatrix(A.n, pin(A.rowptr), pin(A.colind), pin(A.values))
+    X0h = pin(X0)
+    e2e_times, e2e = [], None
+    for i in range(1 + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e = native.solve_csr_host(Ah, X0h, device=local, vectors=True, **dict(common, mode=native.TRL_MODE_FP64))
+        torch.cuda.synchronize()
+        if i > 0:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(statistics.mean(e2e_times))
+
+    # ---- roofline of the dominant kernel class (live, over the timed FP64 solves) ----
+    hbm, bf16, src = peaks()
+    kern = {}
+    for name, s in prof.items():
+        if s["calls"] == 0:
+            continue
+        kern[name] = {"calls": s["calls"], "seconds": s["seconds"], "share": None,
+                      "gbs": s["bytes"] / s["seconds"] / 1e9 if s["seconds"] > 0 else None,
+                      "tflops": s["flops"] / s["seconds"] / 1e12 if s["seconds"] > 0 else None}
+    tot = sum(v["seconds"] for v in kern.values())
+    for v in kern.values():
+        v["share"] = v["seconds"] / tot if tot else None
+    dominant = max(kern, key=lambda k: kern[k]["seconds"])
+    d = kern[dominant]
+    traffic = load_traffic(dominant)
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": d["gbs"], "peak": hbm, "unit": "GB/s", "frac": d["gbs"] / hbm,
+                "traffic": traffic, "peak_source": src}
+    spmm = kern.get("spmm", {})
+
+    result = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(A, X0, o64["restarts"])
+        err64 = float(np.max(np.abs(o64["evals"] - exact) / exact))
+        errmx = float(np.max(np.abs(omx["evals"] - exact) / exact))
+        result = {
+            "metric": METRIC, "value": ms64 / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms64, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "mode": "fp64", "reorth": "block CGS2", "orthonormalize": "CholQR2",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (basis 2.8 GB, CSR 113 MB, per-step working set >> 126 MB)"},
+            "fp64": {"seconds": ms64 / 1e3, "restarts": o64["restarts"], "n_op_apply": o64["n_op_apply"], "converged": bool(o64["converged"]),
+                     "max_rel_residual": o64["max_rel_residual"], "max_rel_err_vs_analytic": err64},
+            "mixed": {"seconds": msmx / 1e3, "speedup_vs_fp64": ms64 / msmx, "restarts_fp32": omx["restarts_fp32"],
+                      "n_op_apply_fp32": omx["n_op_apply_fp32"], "restarts_fp64": omx["restarts"], "n_op_apply_fp64": omx["n_op_apply"],
+                      "seconds_fp32_phase": omx["seconds_fp32"], "fp32_tol": args.fp32_tol, "converged": bool(omx["converged"]),
+                      "max_rel_residual": omx["max_rel_residual"], "max_rel_err_vs_analytic": errmx},
+            "spmm": {"gbs": spmm.get("gbs"), "frac_of_hbm": (spmm.get("gbs") or 0) / hbm, "calls": spmm.get("calls"),
+                     "bytes_per_call": 6137856 * 12 + 4 * 884737 + 2 * 884736 * 8 * 8},
+            "kernels": kern,
+            "roofline": roofline,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(e2e["h2d_bytes"]), "d2h_bytes_per_step": int(e2e["d2h_bytes"]),
+                    "api": "trl_solve_csr_host (pinned host CSR + start block in, eigenvalues + eigenvectors out)"},
+            "gpu_launches": launches // max(1, args.steps) * args.steps,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(result), flush=True)
+    h.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def load_traffic(kernel: str):
+    """DRAM bytes per call from the committed ncu summary of that kernel, if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_baseline(A, X0, restarts_gpu: int):
+    try:
+        from oracle import oracle as O
+    except Exception as e:  # pragma: no cover
+        return {"value": None, "unavailable": str(e)}
+    if not O.available():
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    s = cpu_restart_sample(O, A, X0)
+    try:
+        restarts_ref = load_reference_counts()["restarts"]
+    except Exception:
+        restarts_ref = restarts_gpu
+    return {"value": s["per_restart"] * restarts_ref, "unit": "s", "cores": O.num_threads(), "kind": "reference",
+            "sample": f"reference OpenMP BlockLanczos (ModifiedGS, CholQR) on the same workload: 1 and 2 restart cycles timed "
+                      f"({s['first']:.2f} s, {s['two']:.2f} s); steady-state cycle {s['per_restart']:.3f} s x {restarts_ref} restarts "
+                      f"(the reference's restart count for this workload)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
+    ap.add_argument("--fp32-tol", type=float, default=1e-5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        return
+    trl_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

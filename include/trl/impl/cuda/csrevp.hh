@@ -1,0 +1,102 @@
+#pragma once
+// Sparse operator eigenproblem on the device: Y = alpha*A*X + beta*X with A in full-storage
+// CSR (int32 indices). The CUDA counterpart of the reference's CSREVP examples
+// (examples/openmp/csrevp.hh:19-48, examples/sycl/csrevp.hh:159-187). The shift turns the
+// smallest eigenvalues of A into the largest-magnitude ones of sigma*I - A, which the
+// |theta|-descending ordering of solve_small_dense (evp_base.hh:103) selects.
+//
+// Values are stored in the multivector's Storage type: FP64 for the FP64 backend, FP32 for
+// the mixed-precision backend (whose SpMM runs in FP32 with FP32 accumulation).
+#include "evp_base.hh"
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <type_traits>
+#include <vector>
+
+namespace trl::cuda {
+
+/// Device CSR matrix with values of type V. Owns its arrays when built from host data.
+template <class V>
+class DeviceCSR {
+public:
+  DeviceCSR() = default;
+
+  /// Uploads host CSR arrays (values converted to V).
+  DeviceCSR(std::shared_ptr<Context> ctx, std::int64_t n, std::int64_t nnz, const std::int32_t* rowptr, const std::int32_t* colind, const double* values)
+      : n_(n)
+      , nnz_(nnz)
+  {
+    rowptr_ = DeviceBuffer(ctx, sizeof(std::int32_t) * (n + 1));
+    colind_ = DeviceBuffer(ctx, sizeof(std::int32_t) * (nnz > 0 ? nnz : 1));
+    values_ = DeviceBuffer(ctx, sizeof(V) * (nnz > 0 ? nnz : 1));
+    auto h = ctx->handle();
+    ctx->check(trl_cuda_memcpy(h, rowptr_.get(), rowptr, sizeof(std::int32_t) * (n + 1), TRL_H2D), "CSR upload");
+    if (nnz > 0) {
+      ctx->check(trl_cuda_memcpy(h, colind_.get(), colind, sizeof(std::int32_t) * nnz, TRL_H2D), "CSR upload");
+      if constexpr (std::is_same_v<V, double>) {
+        ctx->check(trl_cuda_memcpy(h, values_.get(), values, sizeof(double) * nnz, TRL_H2D), "CSR upload");
+      }
+      else {
+        std::vector<V> tmp(values, values + nnz);
+        ctx->check(trl_cuda_memcpy(h, values_.get(), tmp.data(), sizeof(V) * nnz, TRL_H2D), "CSR upload");
+        ctx->check(trl_cuda_synchronize(h), "CSR upload");
+      }
+    }
+    desc_ = {n_, nnz_, static_cast<const std::int32_t*>(rowptr_.get()), static_cast<const std::int32_t*>(colind_.get()), values_.get(), dtype_of<V>::value};
+  }
+
+  /// Wraps device arrays owned by the caller.
+  static DeviceCSR wrap(std::int64_t n, std::int64_t nnz, const std::int32_t* rowptr, const std::int32_t* colind, const V* values)
+  {
+    DeviceCSR c;
+    c.n_ = n;
+    c.nnz_ = nnz;
+    c.desc_ = {n, nnz, rowptr, colind, values, dtype_of<V>::value};
+    return c;
+  }
+
+  const trl_csr* desc() const { return &desc_; }
+  std::int64_t rows() const { return n_; }
+  std::int64_t nnz() const { return nnz_; }
+
+private:
+  std::int64_t n_ = 0, nnz_ = 0;
+  DeviceBuffer rowptr_, colind_, values_;
+  trl_csr desc_{};
+};
+
+template <class Storage, unsigned int bs>
+class CSREVP : public EVPBase<Storage, bs> {
+public:
+  using Base = EVPBase<Storage, bs>;
+  using BlockView = typename Base::BlockView;
+
+  CSREVP(std::shared_ptr<Context> ctx, DeviceCSR<Storage> A, double alpha = 1.0, double beta = 0.0)
+      : Base(ctx, static_cast<std::size_t>(A.rows()))
+      , A_(std::move(A))
+      , alpha_(alpha)
+      , beta_(beta)
+  {
+  }
+
+  void apply(BlockView X, BlockView Y) override
+  {
+    this->ctx_->flush();
+    this->ctx_->check(trl_cuda_spmm(this->ctx_->handle(), A_.desc(), Base::dtype, X.data_, Y.data_, bs, alpha_, beta_), "apply");
+    ++applies_;
+  }
+
+  const DeviceCSR<Storage>& matrix() const { return A_; }
+  double alpha() const { return alpha_; }
+  double beta() const { return beta_; }
+  std::uint64_t applies() const { return applies_; }
+
+private:
+  DeviceCSR<Storage> A_;
+  double alpha_, beta_;
+  std::uint64_t applies_ = 0;
+};
+
+} // namespace trl::cuda

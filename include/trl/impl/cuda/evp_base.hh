@@ -1,0 +1,135 @@
+#pragma once
+// Eigenproblem base class of the CUDA backend; the counterpart of trl::openmp::EVPBase
+// (impl/openmp/evp_base.hh:13-181). Everything stays on the device:
+//  - dot              -> trl_cuda_block_dot (FP64 accumulation)                  (:37)
+//  - orthonormalize   -> trl_cuda_cholqr: Cholesky-QR2 by default (one extra pass
+//                        restores orthogonality to working precision); passes = 1
+//                        reproduces the reference's single CholQR                (:39-71)
+//  - solve_small_dense -> trl_cuda_small_eigen: dense FP64 eigensolve of T, sort by
+//                        decreasing |theta|, Ritz-estimate count on the device;
+//                        only the eigenvalues and the count are copied back      (:79-154)
+// The eigenvalues are also kept in host memory because the driver reads them through a
+// host std::span (lanczos.hh:129-131).
+#include "blockmatrix.hh"
+#include "context.hh"
+#include "multivector.hh"
+
+#include <cassert>
+#include <cstddef>
+#include <memory>
+#include <optional>
+#include <span>
+#include <stdexcept>
+#include <vector>
+
+namespace trl::cuda {
+
+template <class Storage, unsigned int block_size>
+class EVPBase {
+public:
+  using Scalar = double;
+  constexpr static auto blocksize = block_size;
+
+  using BlockMultivector = ::trl::cuda::BlockMultivector<Storage, blocksize>;
+  using BlockView = typename BlockMultivector::BlockView;
+  using BlockMatrix = typename BlockMultivector::BlockMatrix;
+  using BlockMatrixBlockView = typename BlockMatrix::BlockView;
+  static constexpr int dtype = dtype_of<Storage>::value;
+
+  EVPBase(std::shared_ptr<Context> ctx, std::size_t n)
+      : ctx_(std::move(ctx))
+      , N(n)
+  {
+  }
+
+  virtual ~EVPBase() = default;
+
+  virtual void apply(BlockView, BlockView) = 0;
+
+  virtual void dot(BlockView V, BlockView W, BlockMatrixBlockView R) { V.dot(W, R); }
+
+  /// True when dot() is the Euclidean inner product; block Gram-Schmidt strategies use the
+  /// multi-block kernels only in that case.
+  virtual bool euclidean_dot() const { return true; }
+
+  virtual void orthonormalize(BlockView V, BlockMatrixBlockView R)
+  {
+    ctx_->flush();
+    ctx_->check(trl_cuda_cholqr(ctx_->handle(), dtype, V.data_, static_cast<std::int64_t>(N), blocksize, cholqr_passes_, R.data_), "orthonormalize");
+  }
+
+  std::size_t size() const { return N; }
+
+  BlockMultivector create_multivector(std::size_t rows, std::size_t cols) const { return BlockMultivector(ctx_, rows, cols); }
+
+  BlockMatrix create_blockmatrix(std::size_t block_rows, std::size_t block_cols) const { return BlockMatrix(ctx_, block_rows, block_cols); }
+
+  virtual std::size_t solve_small_dense(const BlockMatrix& B, BlockMatrixBlockView beta, std::size_t nev)
+  {
+    ctx_->flush();
+    const std::size_t nblk = B.block_rows();
+    const std::size_t n_total = nblk * blocksize;
+    if (!eigenvectors || eigenvectors->block_rows() != nblk) {
+      eigenvectors = std::make_unique<BlockMatrix>(ctx_, nblk, nblk);
+      evals_dev_ = DeviceBuffer(ctx_, sizeof(double) * n_total);
+    }
+    eigenvalues.resize(n_total);
+    int nconv = 0;
+    ctx_->check(trl_cuda_small_eigen(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
+                                     static_cast<double*>(evals_dev_.get()), eigenvectors->data(), eigenvalues.data(), &nconv),
+                "solve_small_dense");
+    return static_cast<std::size_t>(nconv);
+  }
+
+  const std::vector<Scalar>& get_current_eigenvalues() const { return eigenvalues; }
+
+  const BlockMatrix& get_current_eigenvectors() const
+  {
+    assert(eigenvectors);
+    return *eigenvectors;
+  }
+
+  std::span<Scalar, blocksize> get_eigenvalues_block(std::size_t block) { return std::span<Scalar, blocksize>(eigenvalues.data() + block * blocksize, blocksize); }
+
+  void set_tolerance(Scalar tol) { tolerance_ = tol; }
+  Scalar get_tolerance() const { return tolerance_; }
+
+  // ---- backend extensions --------------------------------------------------------------
+
+  /// Number of Cholesky-QR passes in orthonormalize (2 = CholQR2, 1 = reference CholQR).
+  void set_cholqr_passes(int p) { cholqr_passes_ = p; }
+  int cholqr_passes() const { return cholqr_passes_; }
+
+  /// w <- w - V[0:count] (V[0:count]^T w), repeated `passes` times (classical Gram-Schmidt
+  /// against `count` contiguous blocks starting at V0).
+  void project_out(BlockView V0, unsigned int count, BlockView w, int passes)
+  {
+    if (count == 0) return;
+    ctx_->flush();
+    const std::size_t need = sizeof(double) * count * blocksize * blocksize;
+    if (coef_.bytes() < need) coef_ = DeviceBuffer(ctx_, need);
+    auto* C = static_cast<double*>(coef_.get());
+    for (int p = 0; p < passes; ++p) {
+      ctx_->check(trl_cuda_block_dot(ctx_->handle(), dtype, V0.data_, static_cast<int>(count), w.data_, static_cast<std::int64_t>(N), blocksize, C), "project_out dot");
+      ctx_->check(trl_cuda_block_update(ctx_->handle(), dtype, w.data_, V0.data_, static_cast<int>(count), C, static_cast<std::int64_t>(N), blocksize), "project_out update");
+    }
+  }
+
+  Context& context() const { return *ctx_; }
+  const std::shared_ptr<Context>& shared_context() const { return ctx_; }
+  const double* device_eigenvalues() const { return static_cast<const double*>(evals_dev_.get()); }
+
+protected:
+  std::shared_ptr<Context> ctx_;
+  std::size_t N;
+
+  std::vector<Scalar> eigenvalues;
+  std::unique_ptr<BlockMatrix> eigenvectors;
+  DeviceBuffer evals_dev_;
+  DeviceBuffer coef_;
+
+  Scalar tolerance_ = 1e-8;
+  int cholqr_passes_ = 2;
+};
+
+} // namespace trl::cuda

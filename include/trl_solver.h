@@ -1,0 +1,87 @@
+/* trl_solver.h — C entry points that run trl's unchanged BlockLanczos driver
+ * (include/trl/eigensolvers/lanczos.hh in the reference) on the CUDA backend
+ * (include/trl/impl/cuda/, C ABI in trl_cuda.h) for a CSR operator.
+ *
+ * These replace the reference's example driver (examples/openmp/csrtest.cc:90-109: build a
+ * CSR eigenproblem, fill initial_block(), solve(), read get_current_eigenvalues()) for
+ * callers that are not C++ (ctypes, FFI) and add what the driver leaves out: Ritz vectors,
+ * true residuals, per-phase device timings, and the mixed-precision mode.
+ *
+ * Modes
+ *   TRL_MODE_FP64   FP64 basis, FP64 SpMM (the plain backend).
+ *   TRL_MODE_FP32   FP32 basis and FP32 SpMM; Grams, Cholesky, the projected eigenproblem
+ *                   and residuals in FP64. Accuracy is limited by FP32 storage.
+ *   TRL_MODE_MIXED  TRL_MODE_FP32 to fp32_tol, then an FP64 refinement: the FP32 Ritz
+ *                   vectors are rotated out of the FP32 basis, widened to FP64, and a
+ *                   random combination of them starts an FP64 BlockLanczos solve to `tol`.
+ *
+ * The operator is alpha*A + beta*I (alpha = 1, beta = 0 for A itself).
+ * Eigenpairs are returned in the driver's order: decreasing |theta| (evp_base.hh:103).
+ */
+#ifndef TRL_SOLVER_H
+#define TRL_SOLVER_H
+
+#include "trl_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum trl_mode { TRL_MODE_FP64 = 0, TRL_MODE_FP32 = 1, TRL_MODE_MIXED = 2 };
+enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1 };
+
+typedef struct trl_solve_params {
+  int bs;                        /* block size: 1, 2, 4, 8, 16 */
+  int mode;                      /* trl_mode */
+  unsigned nev;                  /* wanted eigenpairs */
+  unsigned ncv;                  /* basis size in vectors (a multiple of bs) */
+  unsigned max_restarts;         /* EigensolverParams::max_restarts (params.hh:8) */
+  double tol;                    /* EigensolverParams::tolerance (params.hh:9) */
+  double alpha, beta;            /* operator alpha*A + beta*I */
+  int reorth;                    /* trl_reorth: reference ModifiedGS or block CGS2 */
+  int cholqr_passes;             /* 1 = CholQR (reference), 2 = CholQR2 */
+  double fp32_tol;               /* TRL_MODE_MIXED: tolerance of the FP32 phase */
+  unsigned refine_max_restarts;  /* TRL_MODE_MIXED: max_restarts of the FP64 phase */
+  int want_vectors;              /* form Ritz vectors and true residuals */
+  int batching;                  /* fuse the restart rotation (see trl::cuda::Context) */
+  unsigned seed;                 /* seed of the refinement's random combination */
+} trl_solve_params;
+
+typedef struct trl_solve_info {
+  int converged;
+  unsigned restarts;        /* restarts of the final phase */
+  unsigned n_op_apply;      /* operator applications of the final phase */
+  unsigned restarts_fp32;   /* TRL_MODE_MIXED: restarts of the FP32 phase */
+  unsigned n_op_apply_fp32; /* TRL_MODE_MIXED: applications of the FP32 phase */
+  double seconds;           /* device time (CUDA events) of the whole solve */
+  double seconds_fp32;      /* device time of the FP32 phase (mixed) */
+  double seconds_vectors;   /* device time of Ritz vectors + residuals */
+  double max_rel_residual;  /* max_c ||op x_c - theta_c x_c|| / ||op||_1 (want_vectors) */
+  double max_theta_residual;/* max_c ||op x_c - theta_c x_c|| / |theta_c| (want_vectors) */
+  double op_norm1;          /* ||op||_1 = max row sum of |alpha*A + beta*I| */
+  unsigned long long kernel_launches; /* kernels launched by the backend during the call */
+  double h2d_bytes, d2h_bytes;        /* host<->device traffic of the call */
+} trl_solve_info;
+
+void trl_solve_params_default(trl_solve_params* p);
+
+/* Host in, host out: uploads the CSR operator and X0 (n x bs row-major), solves, and
+ * returns evals[nev], optionally evecs (n x nev row-major) and resid[nev]
+ * (||op x - theta x|| / ||op||_1). Creates and destroys its own handle on `device`. */
+int trl_solve_csr_host(const trl_solve_params* p, int device, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind, const double* values, const double* X0,
+                       double* evals, double* evecs, double* resid, trl_solve_info* info);
+
+/* Device-resident: A64 (FP64 values) is always needed; A32 (FP32 values of the same
+ * pattern) is used by the FP32 / mixed modes and may be NULL for TRL_MODE_FP64.
+ * X0 is n x bs FP64 on the device. evals_host[nev]; evecs_dev (n x nev row-major FP64,
+ * device) and resid_host[nev] may be NULL. Synchronises the handle's stream on return. */
+int trl_solve_csr_device(trl_cuda_handle h, const trl_solve_params* p, const trl_csr* A64, const trl_csr* A32, const double* X0, double* evals_host, double* evecs_dev,
+                         double* resid_host, trl_solve_info* info);
+
+const char* trl_solver_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TRL_SOLVER_H */

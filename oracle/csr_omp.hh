@@ -1,0 +1,61 @@
+// TEST INFRASTRUCTURE ONLY — part of the CPU oracle. Only tests/, the smoke check and the
+// CPU-baseline leg of bench.py may build, load or run anything under oracle/.
+//
+// CSR operator on the reference OpenMP backend. The reference applies its sparse operator
+// either through Eigen (examples/openmp/csrevp.hh:36-44, lower-triangle selfadjointView) or
+// through a row-per-work-item kernel on full-storage CSR (examples/sycl/csrevp.hh:159-187).
+// Eigen is not installed here, so this follows the full-storage CSR semantics of the latter:
+// Y[r,:] = sum_k val[k] * X[col[k],:] over the row's entries, parallelised over rows.
+// The optional shift (Y = alpha*A*X + beta*X) turns "smallest eigenvalues" into "largest
+// magnitude" for the reference's |theta|-descending ordering (evp_base.hh:103).
+#pragma once
+
+#include <trl/impl/openmp/evp_base.hh>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace trl_oracle {
+
+template <class T, unsigned int bs>
+class CSREVP : public trl::openmp::EVPBase<T, bs> {
+public:
+  using Base = trl::openmp::EVPBase<T, bs>;
+  using BlockView = typename Base::BlockView;
+
+  CSREVP(std::size_t n, const std::int32_t* rowptr, const std::int32_t* colind, const double* values, double alpha = 1.0, double beta = 0.0)
+      : Base(n)
+      , rowptr_(rowptr)
+      , colind_(colind)
+      , values_(values)
+      , alpha_(alpha)
+      , beta_(beta)
+  {
+  }
+
+  void apply(BlockView X, BlockView Y) override
+  {
+    const std::size_t n = this->size();
+    const T* x = X.data_;
+    T* y = Y.data_;
+#pragma omp parallel for schedule(dynamic, 512)
+    for (std::size_t r = 0; r < n; ++r) {
+      T acc[bs] = {};
+      for (std::int32_t k = rowptr_[r]; k < rowptr_[r + 1]; ++k) {
+        const T v = static_cast<T>(values_[k]);
+        const T* xr = x + static_cast<std::size_t>(colind_[k]) * bs;
+#pragma omp simd
+        for (unsigned j = 0; j < bs; ++j) acc[j] += v * xr[j];
+      }
+      for (unsigned j = 0; j < bs; ++j) y[r * bs + j] = static_cast<T>(alpha_) * acc[j] + static_cast<T>(beta_) * x[r * bs + j];
+    }
+  }
+
+private:
+  const std::int32_t* rowptr_;
+  const std::int32_t* colind_;
+  const double* values_;
+  double alpha_, beta_;
+};
+
+} // namespace trl_oracle

@@ -1,0 +1,126 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes access to the CPU oracle (oracle/_ref/liboracle.so).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import
+this module. The library runs the reference's own OpenMP backend (include/trl/impl/openmp/*)
+and its BlockLanczos driver (include/trl/eigensolvers/lanczos.hh), compiled in place with the
+Eigen-free EVPBase restatement in oracle/shim (see oracle/Makefile).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "liboracle.so")
+REF_TESTS = [os.path.join(HERE, "_ref", f"ref_test_lanczos_{t}") for t in ("convergence", "extend")]
+
+# op codes of oracle_block_view_op (reference BlockView methods)
+OP_DOT, OP_MULT, OP_MULT_T, OP_MULT_ADD, OP_SUB_PROD, OP_SUB, OP_COPY, OP_ZERO = range(8)
+
+_lib = None
+
+
+def build(ref: str = "/root/reference") -> None:
+    """Compile oracle/_ref from the reference sources (needs the reference checkout)."""
+    subprocess.run(["make", "-C", HERE, f"REF={ref}", "-j4"], check=True, stdout=subprocess.DEVNULL)
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run `make -C oracle`)")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.oracle_last_error.restype = C.c_char_p
+        L.oracle_solve_csr.argtypes = [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_uint, C.c_double, P, P, P, P, P]
+        L.oracle_block_view_op.argtypes = [C.c_int, C.c_int, C.c_int64, P, P, P]
+        L.oracle_orthonormalize.argtypes = [C.c_int, C.c_int64, P, P]
+        L.oracle_solve_small_dense.argtypes = [C.c_int, C.c_uint, P, P, C.c_uint, C.c_double, P, P, P]
+        L.oracle_spmm.argtypes = [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_double, P, P]
+        L.oracle_symmetric_eigen.argtypes = [C.c_int64, P, P, P]
+        L.oracle_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError("oracle: " + lib().oracle_last_error().decode())
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
+
+
+def solve_csr(A, bs: int, nev: int, ncv: int, X0: np.ndarray, tol: float = 1e-8, max_restarts: int = 1000,
+              alpha: float = 1.0, beta: float = 0.0, ritz: bool = False) -> dict:
+    """Run the reference BlockLanczos (default ModifiedGS) on Y = alpha*A*X + beta*X."""
+    n = A.n
+    X0 = np.ascontiguousarray(X0, dtype=np.float64).reshape(n, bs)
+    evals = np.zeros(ncv)
+    ritz_vecs = np.zeros((n, nev)) if ritz else None
+    stats = np.zeros(3, dtype=np.int32)
+    secs = np.zeros(1)
+    rp = np.ascontiguousarray(A.rowptr, dtype=np.int32)
+    ci = np.ascontiguousarray(A.colind, dtype=np.int32)
+    va = np.ascontiguousarray(A.values, dtype=np.float64)
+    _check(lib().oracle_solve_csr(bs, n, _p(rp), _p(ci), _p(va), alpha, beta, nev, ncv, max_restarts, tol, _p(X0),
+                                  _p(evals), _p(ritz_vecs), _p(stats), _p(secs)))
+    return {"converged": bool(stats[0]), "iterations": int(stats[1]), "n_op_apply": int(stats[2]),
+            "seconds": float(secs[0]), "evals": evals, "ritz": ritz_vecs}
+
+
+def block_view_op(bs: int, op: int, X: np.ndarray, Y: np.ndarray, W: np.ndarray) -> None:
+    n = X.shape[0]
+    _check(lib().oracle_block_view_op(bs, op, n, _p(X), _p(Y), _p(W)))
+
+
+def orthonormalize(V: np.ndarray) -> np.ndarray:
+    n, bs = V.shape
+    R = np.zeros((bs, bs))
+    _check(lib().oracle_orthonormalize(bs, n, _p(V), _p(R)))
+    return R
+
+
+def solve_small_dense(T: np.ndarray, beta: np.ndarray, bs: int, nev: int, tol: float):
+    """T in BlockMatrix layout [nblk][nblk][bs][bs]; returns (evals, evecs-in-block-layout, nconv)."""
+    nblk = T.shape[0]
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    beta = np.ascontiguousarray(beta, dtype=np.float64)
+    evals = np.zeros(nblk * bs)
+    evecs = np.zeros_like(T)
+    nconv = np.zeros(1, dtype=np.int32)
+    _check(lib().oracle_solve_small_dense(bs, nblk, _p(T), _p(beta), nev, tol, _p(evals), _p(evecs), _p(nconv)))
+    return evals, evecs, int(nconv[0])
+
+
+def spmm(A, X: np.ndarray, alpha: float = 1.0, beta: float = 0.0) -> np.ndarray:
+    n, bs = X.shape
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.zeros_like(X)
+    rp = np.ascontiguousarray(A.rowptr, dtype=np.int32)
+    ci = np.ascontiguousarray(A.colind, dtype=np.int32)
+    va = np.ascontiguousarray(A.values, dtype=np.float64)
+    _check(lib().oracle_spmm(bs, n, _p(rp), _p(ci), _p(va), alpha, beta, _p(X), _p(Y)))
+    return Y
+
+
+def symmetric_eigen(A: np.ndarray):
+    n = A.shape[0]
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    w = np.zeros(n)
+    V = np.zeros((n, n))
+    _check(lib().oracle_symmetric_eigen(n, _p(A), _p(w), _p(V)))
+    return w, V

@@ -1,0 +1,116 @@
+"""Host-side logic that needs no GPU.
+
+* trl::cuda::Context's batching of the thick-restart rotation (include/trl/impl/cuda/context.hh)
+  against a fake C ABI: the pattern of lanczos.hh:105-114 becomes one trl_cuda_block_rotate;
+  any other sequence is replayed call by call in its original order.
+* The C-ABI libraries load without a GPU and export every function include/*.h declares.
+* The multi-rank reduction bench.py uses (max over ranks) on a 2-rank gloo group.
+"""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def batching_output(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("host") / "context_batching")
+    src = os.path.join(ROOT, "tests", "host", "context_batching.cc")
+    subprocess.run(["/usr/bin/g++", "-std=c++20", "-O1", f"-I{ROOT}/include", src, "-o", exe], check=True)
+    return subprocess.run([exe], check=True, capture_output=True, text=True).stdout.splitlines()
+
+
+def line(out, key):
+    return next(ln for ln in out if ln.startswith(key + " "))
+
+
+def test_restart_pattern_becomes_one_rotation(batching_output):
+    got = line(batching_output, "case1").split(" ", 2)
+    assert got[1] == "1"
+    assert got[2] == line(batching_output, "expect1").split(" ", 1)[1]
+
+
+def test_irregular_sequences_are_replayed_in_order(batching_output):
+    assert line(batching_output, "case2") == "case2 3 zero | mult 2 | mult 2"
+    assert line(batching_output, "case3") == "case3 1 mult 2"
+    assert line(batching_output, "case4") == "case4 3"
+
+
+def test_single_input_block_and_flush_on_shape_change(batching_output):
+    assert line(batching_output, "case5") == "case5 1 rotate"
+    # the pending single-block group (zero + one mult_add) is itself a k=1, m=1 rotation
+    assert line(batching_output, "case6") == "case6 2 rotate zero"
+    assert line(batching_output, "case7") == "case7 1"
+    assert line(batching_output, "fused") == "fused 3"
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(trl_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_cuda_library_exports_every_declared_symbol():
+    from trl_b200 import native
+
+    lib = ctypes.CDLL(native.CUDA_LIB)
+    names = _declared("trl_cuda.h")
+    assert len(names) >= 30
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) <= set(native.CUDA_SYMBOLS), set(names) - set(native.CUDA_SYMBOLS)
+
+
+def test_solver_library_exports_every_declared_symbol():
+    from trl_b200 import native
+
+    if not os.path.exists(native.SOLVER_LIB):
+        pytest.skip("solver library needs the reference headers at build time")
+    ctypes.CDLL(native.CUDA_LIB, mode=ctypes.RTLD_GLOBAL)
+    lib = ctypes.CDLL(native.SOLVER_LIB)
+    for name in _declared("trl_solver.h"):
+        assert hasattr(lib, name), name
+
+
+def test_status_strings_without_gpu():
+    from trl_b200 import native
+
+    lib = native.cuda_lib()
+    assert lib.trl_cuda_status_string(native.TRL_ECHOLESKY).decode() == "Cholesky factorization failed in orthonormalize"
+    assert lib.trl_cuda_status_string(native.TRL_EEIGEN).decode() == "Eigendecomposition failed"
+
+
+def _max_over_ranks(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    t = torch.tensor([float(rank + 1) * 1.5], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    q.put((rank, float(t.item())))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_max_over_ranks_gloo():
+    import multiprocessing as mp
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_max_over_ranks, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    vals = sorted(q.get(timeout=10) for _ in range(2))
+    assert vals == [(0, 3.0), (1, 3.0)]

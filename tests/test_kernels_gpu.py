@@ -1,0 +1,281 @@
+"""Parity of every C-ABI kernel (include/trl_cuda.h) with the reference's own OpenMP kernels
+(the oracle: impl/openmp/blockview.hh, the restated evp_base.hh) on the same seeded inputs.
+
+Tolerances: FP64 results agree with the reference to 1e-12 relative to the magnitude of the
+summed terms (sum |x_i y_i|); only the summation order differs. FP32 storage is widened to
+FP64 before every product, so contractions of FP32 data agree with an FP64 evaluation of
+the same FP32 inputs to the same 1e-12. FP32 SpMM accumulates in FP32 (as specified for the
+mixed mode) and is held to 1e-5 relative.
+"""
+import numpy as np
+import pytest
+import torch
+
+from trl_b200 import native
+from trl_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+BS = [1, 2, 4, 8, 16]
+DT = [torch.float64, torch.float32]
+
+
+def dev(a, dtype=torch.float64):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.double().cpu().numpy()
+
+
+def as_dt(a, dtype):
+    return a.astype(np.float32).astype(np.float64) if dtype == torch.float32 else a
+
+
+def close(a, b, scale, tol=1e-12):
+    err = np.max(np.abs(a - b)) if a.size else 0.0
+    assert err <= tol * max(scale, 1e-300), (err, scale)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("n", [0, 1, 37, 1029, 200_003])
+def test_dot_matches_reference(cuda_handle, oracle, bs, dtype, n):
+    rng = np.random.default_rng(n * 31 + bs)
+    X = as_dt(rng.standard_normal((n, bs)), dtype)
+    Y = as_dt(rng.standard_normal((n, bs)), dtype)
+    R = np.zeros((bs, bs))
+    oracle.block_view_op(bs, oracle.OP_DOT, X.copy(), Y.copy(), R)  # blockview.hh:152-182
+    Rd = torch.zeros((1, bs, bs), dtype=torch.float64, device="cuda")
+    cuda_handle.block_dot(dev(X, dtype)[None], dev(Y, dtype), Rd)
+    close(host(Rd)[0], R, (np.abs(X).T @ np.abs(Y)).max() if n else 1.0)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("nblk", [1, 3, 9, 17, 49])
+def test_multiblock_dot_and_update(cuda_handle, bs, dtype, nblk):
+    rng = np.random.default_rng(nblk * 7 + bs)
+    n = 4099
+    V = as_dt(rng.standard_normal((nblk, n, bs)), dtype)
+    w = as_dt(rng.standard_normal((n, bs)), dtype)
+    Cd = torch.zeros((nblk, bs, bs), dtype=torch.float64, device="cuda")
+    Vd, wd = dev(V, dtype), dev(w, dtype)
+    cuda_handle.block_dot(Vd, wd, Cd)
+    Cref = np.einsum("jnb,nc->jbc", V, w)
+    close(host(Cd), Cref, np.einsum("jnb,nc->jbc", np.abs(V), np.abs(w)).max())
+    # W -= sum_j V_j C_j  (one classical Gram-Schmidt pass)
+    cuda_handle.block_update(wd, Vd, Cd)
+    ref = w - np.einsum("jnb,jbc->nc", V, host(Cd))
+    got = host(wd)
+    tol = 1e-12 if dtype == torch.float64 else 2e-7
+    close(got, ref, np.abs(ref).max() + np.abs(w).max(), tol)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("n", [1, 13, 5003])
+def test_block_view_ops_match_reference(cuda_handle, oracle, bs, dtype, n):
+    rng = np.random.default_rng(1000 + n + bs)
+    X = as_dt(rng.standard_normal((n, bs)), dtype)
+    Y = as_dt(rng.standard_normal((n, bs)), dtype)
+    W = rng.standard_normal((bs, bs))
+    tol = 1e-12 if dtype == torch.float64 else 2e-7  # FP32 results are rounded to FP32 storage
+    scale = np.abs(X).max() * np.abs(W).sum(axis=0).max() + np.abs(Y).max()
+    Wd = dev(W)
+    # mult: Y = X W  (blockview.hh:104-119)
+    Z = np.zeros_like(X)
+    oracle.block_view_op(bs, oracle.OP_MULT, X.copy(), Z, W.copy())
+    Zd = torch.zeros((n, bs), dtype=dtype, device="cuda")
+    cuda_handle.bv_mult(native.TRL_MULT, dev(X, dtype), Wd, Zd)
+    close(host(Zd), Z, scale, tol)
+    # mult_transpose: Y = X W^T  (blockview.hh:126-141)
+    Z = np.zeros_like(X)
+    oracle.block_view_op(bs, oracle.OP_MULT_T, X.copy(), Z, W.copy())
+    cuda_handle.bv_mult(native.TRL_MULT_TRANSPOSE, dev(X, dtype), Wd, Zd)
+    close(host(Zd), Z, scale, tol)
+    # mult_add: Y += X W  (blockview.hh:81-97)
+    Z = Y.copy()
+    oracle.block_view_op(bs, oracle.OP_MULT_ADD, X.copy(), Z, W.copy())
+    Zd = dev(Y, dtype)
+    cuda_handle.bv_mult(native.TRL_MULT_ADD, dev(X, dtype), Wd, Zd)
+    close(host(Zd), Z, scale, tol)
+    # subtract_product: X -= Y W  (blockview.hh:189-201)
+    Z = X.copy()
+    oracle.block_view_op(bs, oracle.OP_SUB_PROD, Z, Y.copy(), W.copy())
+    Zd = dev(X, dtype)
+    cuda_handle.bv_mult(native.TRL_SUBTRACT, dev(Y, dtype), Wd, Zd)
+    close(host(Zd), Z, scale, tol)
+    # operator-=  (blockview.hh:69-74)
+    Z = X.copy()
+    oracle.block_view_op(bs, oracle.OP_SUB, Z, Y.copy(), W.copy())
+    Zd = dev(X, dtype)
+    cuda_handle.bv_sub(Zd, dev(Y, dtype))
+    close(host(Zd), Z, scale, tol)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("m,k", [(1, 1), (5, 2), (48, 5), (40, 11), (9, 9)])
+def test_rotation_matches_mult_add_loop(cuda_handle, oracle, bs, dtype, m, k):
+    """W_j = sum_i V_i Y_ij in one pass == the k*m mult_add calls of lanczos.hh:105-114."""
+    rng = np.random.default_rng(m * 100 + k + bs)
+    n = 2311
+    V = as_dt(rng.standard_normal((m, n, bs)), dtype)
+    Y = rng.standard_normal((m, m + 1, bs, bs))  # ldy = m + 1 block columns
+    ref = np.zeros((k, n, bs))
+    for j in range(k):
+        for i in range(m):
+            oracle.block_view_op(bs, oracle.OP_MULT_ADD, V[i].copy(), ref[j], Y[i, j].copy())
+    Wd = torch.zeros((k, n, bs), dtype=dtype, device="cuda")
+    cuda_handle.block_rotate(dev(V, dtype), dev(Y), k, Wd)
+    tol = 1e-12 if dtype == torch.float64 else 2e-7
+    close(host(Wd), ref, np.einsum("inb,ijbc->jnc", np.abs(V), np.abs(Y[:, :k])).max(), tol)
+
+
+@pytest.mark.parametrize("bs", BS)
+def test_cholqr_single_pass_matches_reference(cuda_handle, oracle, bs):
+    rng = np.random.default_rng(bs)
+    n = 3001
+    X = rng.standard_normal((n, bs))
+    V = X.copy()
+    R = oracle.orthonormalize(V)  # evp_base.hh:39-71
+    Xd = dev(X)
+    Rd = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+    cuda_handle.cholqr(Xd, 1, Rd)
+    cuda_handle.sync()
+    close(host(Rd), R, np.abs(R).max(), 1e-11)
+    close(host(Xd), V, 1.0, 1e-10)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+def test_cholqr2_orthonormal_and_factor(cuda_handle, bs, dtype):
+    rng = np.random.default_rng(bs + 99)
+    n = 50_000
+    # ill-conditioned block (cond ~ 1e5): CholQR2 restores orthogonality
+    X = rng.standard_normal((n, bs)) @ np.diag(np.logspace(0, -5 if bs > 1 else 0, bs))
+    X = as_dt(X, dtype)
+    Xd = dev(X, dtype)
+    Rd = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+    cuda_handle.cholqr(Xd, 2, Rd)
+    cuda_handle.sync()
+    Q = host(Xd)
+    R = host(Rd)
+    eps = 1e-13 if dtype == torch.float64 else 1e-6
+    assert np.abs(Q.T @ Q - np.eye(bs)).max() < eps * 10
+    assert np.allclose(np.tril(R, -1), 0)
+    rel = np.abs(Q @ R - X).max() / np.abs(X).max()
+    assert rel < (1e-12 if dtype == torch.float64 else 1e-6)
+
+
+def test_cholqr_breakdown_is_reported(cuda_handle):
+    Xd = torch.zeros((100, 4), dtype=torch.float64, device="cuda")
+    Rd = torch.zeros((4, 4), dtype=torch.float64, device="cuda")
+    cuda_handle.cholqr(Xd, 1, Rd)
+    with pytest.raises(native.TrlError) as e:
+        cuda_handle.sync()
+    assert e.value.status == native.TRL_ECHOLESKY
+    cuda_handle.sync()  # the status word is cleared by the report; the context stays usable
+
+
+def _random_csr(n, rng, max_deg=40, empty_frac=0.1):
+    deg = rng.integers(0, max_deg, size=n)
+    deg[rng.random(n) < empty_frac] = 0
+    rows = np.repeat(np.arange(n), deg)
+    cols = rng.integers(0, n, size=rows.size)
+    vals = rng.standard_normal(rows.size)
+    key = np.unique(rows.astype(np.int64) * n + cols)
+    rows, cols = key // n, key % n
+    vals = rng.standard_normal(rows.size)
+    return P._from_coo(n, rows, cols, vals)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 3.5)])
+def test_spmm_matches_reference(cuda_handle, oracle, bs, alpha, beta):
+    rng = np.random.default_rng(bs)
+    for A in (P.laplace2d(64), _random_csr(7919, rng), P.diagonal(5)):
+        X = rng.standard_normal((A.n, bs))
+        ref = oracle.spmm(A, X, alpha, beta)  # examples/sycl/csrevp.hh:159-187 semantics
+        Ad = native.DeviceCSRTensors.from_host(A)
+        Yd = torch.zeros((A.n, bs), dtype=torch.float64, device="cuda")
+        cuda_handle.spmm(Ad, dev(X), Yd, alpha, beta)
+        rows = A.row_indices()
+        mag = np.zeros(A.n)
+        np.add.at(mag, rows, np.abs(A.values) * np.abs(X[A.colind]).max(axis=1))
+        close(host(Yd), ref, mag.max() + abs(beta) * np.abs(X).max())
+
+
+@pytest.mark.parametrize("bs", [4, 8, 16])
+def test_spmm_fp32(cuda_handle, oracle, bs):
+    rng = np.random.default_rng(5)
+    A = _random_csr(10007, rng, max_deg=100)
+    X = rng.standard_normal((A.n, bs)).astype(np.float32).astype(np.float64)
+    ref = oracle.spmm(A, X)
+    Ad = native.DeviceCSRTensors.from_host(A, torch.float32)
+    Yd = torch.zeros((A.n, bs), dtype=torch.float32, device="cuda")
+    cuda_handle.spmm(Ad, dev(X, torch.float32), Yd)
+    scale = np.abs(ref).max()
+    close(host(Yd), ref, scale, 1e-5)
+
+
+def test_spmm_rejects_bad_arguments(cuda_handle):
+    A = native.DeviceCSRTensors.from_host(P.laplace1d(16))
+    X = torch.zeros((16, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(native.TrlError) as e:
+        cuda_handle.spmm(A, X, torch.zeros_like(X))
+    assert e.value.status == native.TRL_ENOTSUP
+    X = torch.zeros((16, 4), dtype=torch.float64, device="cuda")
+    with pytest.raises(native.TrlError) as e:
+        cuda_handle.spmm(A, X, X)
+    assert e.value.status == native.TRL_EINVAL
+
+
+@pytest.mark.parametrize("bs,nblk", [(1, 7), (4, 10), (8, 12), (16, 4)])
+def test_small_eigen_matches_reference(cuda_handle, oracle, bs, nblk):
+    rng = np.random.default_rng(bs * nblk)
+    N = bs * nblk
+    M = rng.standard_normal((N, N))
+    D = M + M.T
+    # block layout with a garbage upper triangle: both implementations read the lower one
+    T = D.reshape(nblk, bs, nblk, bs).transpose(0, 2, 1, 3).copy()
+    beta = np.triu(rng.standard_normal((bs, bs))) * 1e-7
+    nev = min(N, 2 * bs + 1)
+    ev_ref, Y_ref, nc_ref = oracle.solve_small_dense(T, beta, bs, nev, tol=1e-7)
+    evals, evecs, ev_host, nconv = cuda_handle.small_eigen(dev(T), dev(beta), nev, 1e-7)
+    assert np.allclose(ev_host, ev_ref, rtol=0, atol=1e-12 * np.abs(ev_ref).max())
+    assert np.allclose(host(evals), ev_host)
+    Yg = host(evecs).transpose(0, 2, 1, 3).reshape(N, N)
+    Yr = Y_ref.transpose(0, 2, 1, 3).reshape(N, N)
+    signs = np.sign(np.sum(Yg * Yr, axis=0))
+    assert np.allclose(Yg * signs, Yr, atol=1e-10)
+    assert nconv == nc_ref
+
+
+def test_sddmm_matches_dense(cuda_handle):
+    rng = np.random.default_rng(11)
+    A = _random_csr(3001, rng)
+    k = 5
+    X = rng.standard_normal((A.n, k))
+    w = rng.uniform(size=k)
+    out = torch.zeros(A.nnz, dtype=torch.float64, device="cuda")
+    cuda_handle.sddmm(native.DeviceCSRTensors.from_host(A), dev(X), dev(w), out)
+    rows = A.row_indices()
+    ref = np.sum(w * X[rows] * X[A.colind], axis=1)
+    close(host(out), ref, np.abs(ref).max() + 1e-300)
+
+
+def test_convert_and_norm1(cuda_handle):
+    A = P.anisotropic3d(8)
+    Ad = native.DeviceCSRTensors.from_host(A)
+    assert cuda_handle.csr_norm1(Ad) == pytest.approx(A.gershgorin_bound(), rel=1e-15)
+    sig = 500.0
+    assert cuda_handle.csr_norm1(Ad, -1.0, sig) == pytest.approx(
+        np.max(np.abs(sig - np.diag(A.to_dense())) + np.abs(A.to_dense() - np.diag(np.diag(A.to_dense()))).sum(1)), rel=1e-14)
+    x = torch.randn(1000, dtype=torch.float64, device="cuda")
+    y = torch.empty(1000, dtype=torch.float32, device="cuda")
+    cuda_handle.convert(y, x)
+    torch.cuda.synchronize()
+    assert torch.equal(y, x.float())

@@ -1,0 +1,154 @@
+"""End-to-end parity of the CUDA backend driven by the reference's unchanged BlockLanczos.
+
+* The reference's own test bodies (tests/test_lanczos_{convergence,extend}.hh) run on the
+  CUDA backend (trl_b200/lib/trl_cuda_ref_tests) with the reference's cases and tolerances.
+* The small benchmark workload (2-D 5-point Laplacian 128x128, bs 4, nev 10, ncv 160) is
+  solved by the oracle (reference OpenMP backend) and by the CUDA backend from the same
+  start block: eigenvalues agree to 1e-10 relative, eigenvector subspaces by principal
+  angles per eigenvalue cluster, residuals ||Ax - lambda x|| / ||A||_1 below the tolerance.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+import torch
+
+from trl_b200 import native
+from trl_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(args):
+    return subprocess.run(args, capture_output=True, text=True, timeout=600)
+
+
+def test_reference_test_bodies_fp64():
+    r = _run([native.REF_TESTS_BIN])
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert "ALL PASSED" in r.stdout
+    assert r.stdout.count(" passed.") == 8 and r.stdout.count("Passed.") == 4
+
+
+def test_reference_test_bodies_fp32():
+    r = _run([native.REF_TESTS_BIN, "fp32"])
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    assert "ALL PASSED" in r.stdout
+
+
+def clusters(evals, rel=1e-8):
+    groups, cur = [], [0]
+    for i in range(1, len(evals)):
+        if abs(evals[i] - evals[i - 1]) <= rel * abs(evals[0]):
+            cur.append(i)
+        else:
+            groups.append(cur)
+            cur = [i]
+    groups.append(cur)
+    return groups
+
+
+def max_principal_sine(Xa, Xb, evals):
+    """max over eigenvalue clusters of sin(largest principal angle) between the two spans."""
+    worst = 0.0
+    for g in clusters(evals):
+        Qa, _ = np.linalg.qr(Xa[:, g])
+        Qb, _ = np.linalg.qr(Xb[:, g])
+        s = np.linalg.norm(Qb - Qa @ (Qa.T @ Qb), 2)
+        worst = max(worst, s)
+    return worst
+
+
+@pytest.fixture(scope="module")
+def cfg1_oracle(oracle):
+    A = P.laplace2d(128)
+    X0 = P.initial_block(A.n, 4, seed=42)
+    r = oracle.solve_csr(A, 4, 10, 160, X0, tol=1e-8, ritz=True)
+    assert r["converged"]
+    return A, X0, r
+
+
+@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS2, native.TRL_REORTH_MGS])
+@pytest.mark.parametrize("passes", [1, 2])
+def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
+    A, X0, ref = cfg1_oracle
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8, reorth=reorth, cholqr_passes=passes)
+    assert out["converged"]
+    exact = P.laplace2d_eigenvalues(128)[:10]
+    assert np.max(np.abs(out["evals"] - ref["evals"][:10]) / np.abs(ref["evals"][:10])) < 1e-10
+    assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-10
+    # the Ritz estimate test is ||beta y|| / |theta| < tol; true residuals sit at that level
+    assert out["max_theta_residual"] < 5e-8
+    assert np.max(out["resid"]) < 5e-8
+    assert max_principal_sine(out["evecs"], ref["ritz"], out["evals"]) < 1e-5
+    # same number of restarts as the reference up to small drift from rounding
+    assert abs(out["restarts"] - ref["iterations"]) <= max(3, ref["iterations"] // 5)
+
+
+def test_cfg1_mixed_reaches_fp64_accuracy(cfg1_oracle):
+    A, X0, ref = cfg1_oracle
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-5)
+    assert out["converged"]
+    exact = P.laplace2d_eigenvalues(128)[:10]
+    assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-11
+    assert out["max_rel_residual"] < 1e-9
+    assert out["restarts_fp32"] > 0
+
+
+def test_fp32_mode_accuracy_is_stated(cfg1_oracle):
+    A, X0, ref = cfg1_oracle
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-5, mode=native.TRL_MODE_FP32)
+    assert out["converged"]
+    exact = P.laplace2d_eigenvalues(128)[:10]
+    assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-5
+
+
+def test_device_entry_point_matches_host_entry_point(cfg1_oracle):
+    A, X0, ref = cfg1_oracle
+    h = native.Handle(0)
+    A64 = native.DeviceCSRTensors.from_host(A)
+    X0d = torch.from_numpy(X0).cuda()
+    ev = torch.zeros((A.n, 10), dtype=torch.float64, device="cuda")
+    out = native.solve_csr_device(h, A64, None, X0d, evecs=ev, bs=4, nev=10, ncv=160, tol=1e-8)
+    host = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8)
+    assert out["converged"] and host["converged"]
+    assert np.allclose(out["evals"], host["evals"], rtol=1e-13)
+    assert out["kernel_launches"] > 0
+    h.close()
+
+
+def test_smallest_via_shift(oracle):
+    """Smallest eigenvalues through sigma*I - A (the |theta|-descending order keeps largest)."""
+    A = P.anisotropic3d(12, coef=(1.0, 2.0, 3.0))
+    sigma = A.gershgorin_bound()
+    X0 = P.initial_block(A.n, 4, seed=1)
+    out = native.solve_csr_host(A, X0, bs=4, nev=8, ncv=64, tol=1e-10, alpha=-1.0, beta=sigma)
+    lam = sigma - out["evals"]
+    exact = np.sort(np.linalg.eigvalsh(A.to_dense()))[:8]
+    assert np.max(np.abs(lam - exact) / np.abs(exact)) < 1e-9
+    ref = oracle.solve_csr(A, 4, 8, 64, X0, tol=1e-10, alpha=-1.0, beta=sigma)
+    assert np.max(np.abs(out["evals"] - ref["evals"][:8]) / ref["evals"][:8]) < 1e-10
+
+
+def test_invalid_parameters_raise():
+    A = P.laplace1d(64)
+    X0 = P.initial_block(64, 4)
+    with pytest.raises(native.TrlError) as e:
+        native.solve_csr_host(A, X0, bs=4, nev=16, ncv=16)  # nev >= ncv (lanczos.hh:50)
+    assert e.value.status == native.TRL_EINVAL
+    with pytest.raises(native.TrlError):
+        native.solve_csr_host(A, X0, bs=4, nev=4, ncv=62)  # ncv not a multiple of bs
+
+
+@pytest.mark.slow
+def test_cfg2_fp64_and_mixed_to_analytic():
+    """The 96^3 anisotropic Laplacian (1,10,100): 32 largest to 1e-10, both modes."""
+    A = P.anisotropic3d(96)
+    exact = P.anisotropic3d_eigenvalues(96, k=32)
+    X0 = P.initial_block(A.n, 8, seed=42)
+    for mode in (native.TRL_MODE_FP64, native.TRL_MODE_MIXED):
+        out = native.solve_csr_host(A, X0, vectors=False, bs=8, nev=32, ncv=384, tol=1e-10, mode=mode, fp32_tol=1e-5)
+        assert out["converged"], mode
+        assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-10, mode
+        assert out["max_rel_residual"] < 1e-9, mode

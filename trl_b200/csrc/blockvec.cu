@@ -1,0 +1,616 @@
+// Block-vector kernels of the backend: elementwise ops, the multi-block inner product
+// (block dot), the tall-skinny block GEMM behind mult / mult_transpose / mult_add /
+// subtract_product / the CGS projection update / the thick-restart rotation, and
+// Cholesky-QR. Contractions run on the FP64 tensor cores (DMMA m8n8k4); FP32 storage is
+// widened to FP64 in registers, so products are exact and sums are FP64.
+//
+// Layout: a block vector is n x BS row-major; block j of a multivector at base + j*n*BS.
+#include "common.cuh"
+
+namespace {
+
+constexpr int kThreads = 256; // 8 warps per CTA for every kernel in this file
+constexpr int kWarps = kThreads / 32;
+
+// ---------------------------------------------------------------- elementwise
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int width = 2;
+};
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int width = 4;
+};
+
+template <typename T>
+__device__ __forceinline__ void vsub(typename Vec16<T>::type& a, const typename Vec16<T>::type& b);
+template <>
+__device__ __forceinline__ void vsub<double>(double2& a, const double2& b)
+{
+  a.x -= b.x;
+  a.y -= b.y;
+}
+template <>
+__device__ __forceinline__ void vsub<float>(float4& a, const float4& b)
+{
+  a.x -= b.x;
+  a.y -= b.y;
+  a.z -= b.z;
+  a.w -= b.w;
+}
+
+// X -= Y over `count` elements; vectorised when both pointers are 16-byte aligned.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_sub(T* __restrict__ X, const T* __restrict__ Y, int64_t count, int vec_ok)
+{
+  const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::width;
+  int64_t done = 0;
+  if (vec_ok) {
+    const int64_t nv = count / W;
+    V* xv = reinterpret_cast<V*>(X);
+    const V* yv = reinterpret_cast<const V*>(Y);
+    for (int64_t i = tid; i < nv; i += stride) {
+      V a = xv[i];
+      vsub<T>(a, yv[i]);
+      xv[i] = a;
+    }
+    done = nv * W;
+  }
+  for (int64_t i = done + tid; i < count; i += stride) X[i] -= Y[i];
+}
+
+template <typename D, typename S>
+__global__ void __launch_bounds__(kThreads) k_convert(D* __restrict__ dst, const S* __restrict__ src, int64_t count)
+{
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) dst[i] = static_cast<D>(src[i]);
+}
+
+// ---------------------------------------------------------------- block dot
+// C_j = V_j^T W, j < nblk. Grid: x = chunk of JC blocks, y = chunk of rows.
+// A warp takes G groups of 4 rows per iteration. All operand loads of the iteration are
+// issued before the first DMMA (block indices beyond nblk are clamped to a valid block and
+// their products discarded), so each warp keeps G*(JC+1)*NT 256-byte loads in flight.
+// Per group: one DMMA m8n8k4 per (j, 8x8 output tile). Per-CTA sums go to
+// partial[row_chunk][j][BS*BS]; k_reduce_partials adds the row chunks in a fixed order.
+template <typename T, int BS, int JC, int G>
+__global__ void __launch_bounds__(kThreads) k_block_dot(const T* __restrict__ V, int64_t vstride, int nblk, const T* __restrict__ W, int64_t n, int64_t rows_per_cta,
+                                                        double* __restrict__ partial)
+{
+  constexpr int NT = (BS + 7) / 8;
+  constexpr int BB = BS * BS;
+  __shared__ double red[kWarps][NT * NT * 64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int j0 = blockIdx.x * JC;
+  const int64_t rb = static_cast<int64_t>(blockIdx.y) * rows_per_cta;
+  const int64_t re = min(n, rb + rows_per_cta);
+
+  double acc[JC][NT][NT][2];
+#pragma unroll
+  for (int jj = 0; jj < JC; ++jj)
+#pragma unroll
+    for (int a = 0; a < NT; ++a)
+#pragma unroll
+      for (int b = 0; b < NT; ++b) acc[jj][a][b][0] = acc[jj][a][b][1] = 0.0;
+
+  const T* Vb[JC];
+#pragma unroll
+  for (int jj = 0; jj < JC; ++jj) Vb[jj] = V + static_cast<int64_t>(min(j0 + jj, nblk - 1)) * vstride;
+
+  for (int64_t r0 = rb + warp * 4 * G; r0 < re; r0 += kWarps * 4 * G) {
+    double bf[G][NT];
+    double av[G][JC][NT];
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+      const int64_t row = r0 + q * 4 + t4;
+      const bool rok = row < re;
+#pragma unroll
+      for (int tk = 0; tk < NT; ++tk) {
+        const int col = tk * 8 + g;
+        bf[q][tk] = (rok && col < BS) ? ld_widen(W + row * BS + col) : 0.0;
+      }
+#pragma unroll
+      for (int jj = 0; jj < JC; ++jj)
+#pragma unroll
+        for (int ti = 0; ti < NT; ++ti) {
+          const int col = ti * 8 + g;
+          av[q][jj][ti] = (rok && col < BS) ? ld_widen(Vb[jj] + row * BS + col) : 0.0;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < G; ++q)
+#pragma unroll
+      for (int jj = 0; jj < JC; ++jj) {
+        if (j0 + jj < nblk) {
+#pragma unroll
+          for (int ti = 0; ti < NT; ++ti)
+#pragma unroll
+            for (int tk = 0; tk < NT; ++tk) dmma_m8n8k4(acc[jj][ti][tk][0], acc[jj][ti][tk][1], av[q][jj][ti], bf[q][tk]);
+        }
+      }
+  }
+
+  // cross-warp reduction, one block j at a time
+#pragma unroll
+  for (int jj = 0; jj < JC; ++jj) {
+    if (j0 + jj >= nblk) break;
+#pragma unroll
+    for (int ti = 0; ti < NT; ++ti)
+#pragma unroll
+      for (int tk = 0; tk < NT; ++tk) {
+        red[warp][(ti * NT + tk) * 64 + g * 8 + 2 * t4 + 0] = acc[jj][ti][tk][0];
+        red[warp][(ti * NT + tk) * 64 + g * 8 + 2 * t4 + 1] = acc[jj][ti][tk][1];
+      }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NT * NT * 64; e += kThreads) {
+      const int tile = e >> 6, within = e & 63;
+      const int row = (tile / NT) * 8 + (within >> 3);
+      const int col = (tile % NT) * 8 + (within & 7);
+      if (row < BS && col < BS) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s += red[w][e];
+        partial[(static_cast<int64_t>(blockIdx.y) * nblk + j0 + jj) * BB + row * BS + col] = s;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// out[e] = sum_c partial[c][e]: 32 outputs per CTA, 8 slices of the chunk range per output
+// with four independent accumulators each (the loads overlap), combined in a fixed order.
+__global__ void __launch_bounds__(kThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out)
+{
+  __shared__ double part[8][33];
+  const int o = threadIdx.x & 31, s = threadIdx.x >> 5;
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + o;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  if (e < len) {
+    int c = s;
+    for (; c + 24 < chunks; c += 32) {
+      a0 += partial[static_cast<int64_t>(c) * len + e];
+      a1 += partial[static_cast<int64_t>(c + 8) * len + e];
+      a2 += partial[static_cast<int64_t>(c + 16) * len + e];
+      a3 += partial[static_cast<int64_t>(c + 24) * len + e];
+    }
+    for (; c < chunks; c += 8) a0 += partial[static_cast<int64_t>(c) * len + e];
+  }
+  part[s][o] = (a0 + a1) + (a2 + a3);
+  __syncthreads();
+  if (s == 0 && e < len) {
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t += part[q][o];
+    out[e] = t;
+  }
+}
+
+// ---------------------------------------------------------------- block GEMM
+// out_j = (accumulate ? out_j : 0) + sign * sum_{i<MB} in_i * Coef(i, j)   for j < NB <= NBMAX
+// Coef(i, j) = coef + (i*ldc + j)*BS*BS (row-major BS x BS, or its transpose).
+// A warp owns RT 8-row tiles at a time and walks the input blocks U at a time: the
+// A-fragment loads of U blocks x RT tiles (from `in`, HBM) are all issued before the DMMAs
+// that consume them (indices past MB are clamped and their products skipped). B fragments
+// come from the tiny coefficient array (L1-resident) and are shared by the RT tiles.
+// `in` and `out` may alias when MB = NB = 1 (in-place X <- X U^{-1}): a warp reads all its
+// rows before it writes them, and no other warp touches those rows.
+template <typename T, int BS, int NBMAX, int RT, int U>
+__global__ void __launch_bounds__(kThreads) k_block_gemm(const T* in, int64_t istride, int MB, const double* __restrict__ coef, int ldc, int transpose_coef, T* out,
+                                                         int64_t ostride, int NB, int64_t n, int accumulate, double sign)
+{
+  constexpr int NT = (BS + 7) / 8;
+  constexpr int KS = (BS + 3) / 4;
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5);
+  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * kWarps;
+
+  for (int64_t r0 = warp_global * 8 * RT; r0 < n; r0 += warp_stride * 8 * RT) {
+    double acc[RT][NBMAX][NT][2];
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+      const int64_t row = r0 + r * 8 + g;
+      const bool rok = row < n;
+#pragma unroll
+      for (int jb = 0; jb < NBMAX; ++jb)
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int col = t * 8 + 2 * t4 + i;
+            acc[r][jb][t][i] = (accumulate && jb < NB && rok && col < BS) ? static_cast<double>(out[jb * ostride + row * BS + col]) : 0.0;
+          }
+    }
+
+    for (int ib0 = 0; ib0 < MB; ib0 += U) {
+      double a[U][RT][KS];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const T* A = in + static_cast<int64_t>(min(ib0 + u, MB - 1)) * istride;
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+          const int64_t row = r0 + r * 8 + g;
+#pragma unroll
+          for (int ks = 0; ks < KS; ++ks) {
+            const int kcol = ks * 4 + t4;
+            a[u][r][ks] = (row < n && kcol < BS) ? static_cast<double>(A[row * BS + kcol]) : 0.0;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (ib0 + u < MB) {
+          const double* Crow = coef + static_cast<int64_t>(ib0 + u) * ldc * (BS * BS);
+#pragma unroll
+          for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+            for (int jb = 0; jb < NBMAX; ++jb) {
+              if (jb < NB) {
+                const double* Cb = Crow + jb * (BS * BS);
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                  const int krow = ks * 4 + t4, ncol = t * 8 + g;
+                  double b = 0.0;
+                  if (krow < BS && ncol < BS) b = sign * __ldg(transpose_coef ? Cb + ncol * BS + krow : Cb + krow * BS + ncol);
+#pragma unroll
+                  for (int r = 0; r < RT; ++r) dmma_m8n8k4(acc[r][jb][t][0], acc[r][jb][t][1], a[u][r][ks], b);
+                }
+              }
+            }
+        }
+      }
+    }
+
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+      const int64_t row = r0 + r * 8 + g;
+#pragma unroll
+      for (int jb = 0; jb < NBMAX; ++jb)
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int col = t * 8 + 2 * t4 + i;
+            if (jb < NB && row < n && col < BS) out[jb * ostride + row * BS + col] = static_cast<T>(acc[r][jb][t][i]);
+          }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- small Cholesky
+// G = U^T U (lower triangle of G read, as an LL^T factorisation); writes U^{-1} for the
+// apply and folds U into R (R <- U on the first pass, R <- U R afterwards, so that
+// X_in = X_out R across passes). A pivot <= 0 records TRL_DEV_CHOLESKY and writes the
+// identity so that the apply leaves X unchanged.
+template <int BS>
+__global__ void k_chol_factor(const double* __restrict__ G, double* __restrict__ Uinv, double* __restrict__ R, int first, int* status)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double L[BS][BS];
+  bool ok = true;
+  for (int j = 0; j < BS && ok; ++j) {
+    double d = G[j * BS + j];
+    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+    if (!(d > 0.0)) {
+      ok = false;
+      break;
+    }
+    const double ljj = sqrt(d);
+    L[j][j] = ljj;
+    for (int i = j + 1; i < BS; ++i) {
+      double s = G[i * BS + j];
+      for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+      L[i][j] = s / ljj;
+    }
+    for (int i = 0; i < j; ++i) L[i][j] = 0.0;
+  }
+  if (!ok) {
+    atomicOr(status, TRL_DEV_CHOLESKY);
+    for (int i = 0; i < BS * BS; ++i) Uinv[i] = (i / BS == i % BS) ? 1.0 : 0.0;
+    return;
+  }
+  // U = L^T; inverse of U by back substitution, column by column
+  double Ui[BS][BS];
+  for (int c = 0; c < BS; ++c) {
+    for (int i = BS - 1; i >= 0; --i) {
+      if (i > c) {
+        Ui[i][c] = 0.0;
+        continue;
+      }
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = i + 1; k <= c; ++k) s -= L[k][i] * Ui[k][c]; // U[i][k] = L[k][i]
+      Ui[i][c] = s / L[i][i];
+    }
+  }
+  for (int i = 0; i < BS; ++i)
+    for (int c = 0; c < BS; ++c) Uinv[i * BS + c] = Ui[i][c];
+  if (first) {
+    for (int i = 0; i < BS; ++i)
+      for (int c = 0; c < BS; ++c) R[i * BS + c] = (c >= i) ? L[c][i] : 0.0;
+  }
+  else {
+    double Rn[BS][BS];
+    for (int i = 0; i < BS; ++i)
+      for (int c = 0; c < BS; ++c) {
+        double s = 0.0;
+        for (int k = i; k <= c; ++k) s += L[k][i] * R[k * BS + c];
+        Rn[i][c] = (c >= i) ? s : 0.0;
+      }
+    for (int i = 0; i < BS; ++i)
+      for (int c = 0; c < BS; ++c) R[i * BS + c] = Rn[i][c];
+  }
+}
+
+} // namespace
+
+using namespace trl_detail;
+
+// ---------------------------------------------------------------- launchers
+namespace trl_detail {
+
+template <typename T, int BS, int JC, int G>
+int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C)
+{
+  const int64_t len = static_cast<int64_t>(nblk) * BS * BS;
+  const int gj = (nblk + JC - 1) / JC;
+  // about 4 CTAs per SM in total, 512+ rows per CTA
+  int64_t target = static_cast<int64_t>(h->num_sms) * 4 / gj;
+  if (target < 1) target = 1;
+  int64_t max_chunks = (n + 511) / 512;
+  int64_t chunks = target < max_chunks ? target : max_chunks;
+  if (chunks < 1) chunks = 1;
+  int64_t rows_per_cta = (n + chunks - 1) / chunks;
+  constexpr int step = kWarps * 4 * G; // rows one CTA iteration covers
+  rows_per_cta = (rows_per_cta + step - 1) / step * step;
+  chunks = (n + rows_per_cta - 1) / rows_per_cta;
+  double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
+  if (!partial) return TRL_ENOMEM;
+  dim3 grid(gj, static_cast<unsigned>(chunks));
+  k_block_dot<T, BS, JC, G><<<grid, kThreads, 0, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial);
+  int st = after_launch(h, "block_dot");
+  if (st) return st;
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C);
+  return after_launch(h, "block_dot reduce");
+}
+
+// Chooses the block chunk JC (accumulators per warp) and the row groups G per iteration so
+// that every warp keeps about 16-20 independent loads in flight.
+template <typename T, int BS>
+int launch_block_dot(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C)
+{
+  if (n == 0) {
+    cudaMemsetAsync(C, 0, static_cast<size_t>(nblk) * BS * BS * sizeof(double), h->stream);
+    return TRL_OK;
+  }
+  if (nblk == 1) return launch_block_dot_jc<T, BS, 1, 8>(h, V, nblk, W, n, C);
+  if (nblk == 2) return launch_block_dot_jc<T, BS, 2, 4>(h, V, nblk, W, n, C);
+  if (nblk <= 4) return launch_block_dot_jc<T, BS, 4, (BS >= 16 ? 2 : 4)>(h, V, nblk, W, n, C);
+  return launch_block_dot_jc<T, BS, (BS >= 16 ? 4 : 8), 2>(h, V, nblk, W, n, C);
+}
+
+template <typename T, int BS, int NBMAX>
+void launch_gemm_nb(trl_cuda_context* h, const T* in, int MB, const double* coef, int ldc, int transpose, T* out, int nb, int64_t n, int accumulate, double sign)
+{
+  constexpr int NT = (BS + 7) / 8;
+  constexpr int KS = (BS + 3) / 4;
+  constexpr int RT = (NBMAX * NT >= 8) ? 1 : 2; // keep the accumulators within ~64 registers
+  constexpr int U = (KS >= 4) ? 2 : 4;
+  const unsigned grid = grid_for(h, (n + 8 * RT - 1) / (8 * RT), kWarps, 8);
+  k_block_gemm<T, BS, NBMAX, RT, U><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
+}
+
+template <typename T, int BS>
+int launch_block_gemm(trl_cuda_context* h, const T* in, int MB, const double* coef, int ldc, int transpose, T* out, int NB, int64_t n, int accumulate, double sign)
+{
+  if (n == 0 || NB == 0) return TRL_OK;
+  constexpr int NBCAP = (BS >= 16) ? 4 : 16;
+  for (int j0 = 0; j0 < NB; j0 += NBCAP) {
+    const int nb = (NB - j0) < NBCAP ? (NB - j0) : NBCAP;
+    const double* cj = coef + static_cast<int64_t>(j0) * BS * BS;
+    T* oj = out + static_cast<int64_t>(j0) * n * BS;
+    if (nb == 1)
+      launch_gemm_nb<T, BS, 1>(h, in, MB, cj, ldc, transpose, oj, nb, n, accumulate, sign);
+    else if (nb <= 2)
+      launch_gemm_nb<T, BS, 2>(h, in, MB, cj, ldc, transpose, oj, nb, n, accumulate, sign);
+    else if (nb <= 4)
+      launch_gemm_nb<T, BS, 4>(h, in, MB, cj, ldc, transpose, oj, nb, n, accumulate, sign);
+    else if (nb <= 8)
+      launch_gemm_nb<T, BS, 8>(h, in, MB, cj, ldc, transpose, oj, nb, n, accumulate, sign);
+    else
+      launch_gemm_nb<T, BS, NBCAP>(h, in, MB, cj, ldc, transpose, oj, nb, n, accumulate, sign);
+    int st = after_launch(h, "block_gemm");
+    if (st) return st;
+  }
+  return TRL_OK;
+}
+
+} // namespace trl_detail
+
+static int check_common(trl_cuda_context* h, int dtype, int64_t n, int bs)
+{
+  if (!valid_dtype(dtype)) return set_error(h, TRL_ENOTSUP, "unsupported dtype %d", dtype);
+  if (!valid_bs(bs)) return set_error(h, TRL_ENOTSUP, "unsupported block size %d", bs);
+  if (n < 0) return set_error(h, TRL_EINVAL, "negative row count");
+  return TRL_OK;
+}
+
+static size_t elt_size(int dtype) { return dtype == TRL_F64 ? sizeof(double) : sizeof(float); }
+
+extern "C" {
+
+int trl_cuda_bv_zero(trl_cuda_handle h, int dtype, void* X, int64_t n, int bs)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  ProfScope prof(h, PROF_COPY, static_cast<double>(n) * bs * elt_size(dtype));
+  return trl_cuda_memset_zero(h, X, static_cast<size_t>(n) * bs * elt_size(dtype));
+}
+
+int trl_cuda_bv_copy(trl_cuda_handle h, int dtype, void* X, const void* Y, int64_t n, int bs)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (X == Y) return TRL_OK;
+  ProfScope prof(h, PROF_COPY, 2.0 * n * bs * elt_size(dtype));
+  return trl_cuda_memcpy(h, X, Y, static_cast<size_t>(n) * bs * elt_size(dtype), TRL_D2D);
+}
+
+int trl_cuda_bv_sub(trl_cuda_handle h, int dtype, void* X, const void* Y, int64_t n, int bs)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  const int64_t count = n * bs;
+  if (count == 0) return TRL_OK;
+  if (!X || !Y) return set_error(h, TRL_EINVAL, "null pointer");
+  ProfScope prof(h, PROF_SUB, 3.0 * count * elt_size(dtype));
+  const int vec_ok = ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 15) == 0;
+  const unsigned grid = grid_for(h, count / 4 + 1, kThreads, 8);
+  TRL_DISPATCH_DT(dtype, k_sub<T><<<grid, kThreads, 0, h->stream>>>(static_cast<T*>(X), static_cast<const T*>(Y), count, vec_ok));
+  return after_launch(h, "bv_sub");
+}
+
+int trl_cuda_convert(trl_cuda_handle h, int dst_dtype, void* dst, int src_dtype, const void* src, int64_t count)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!valid_dtype(dst_dtype) || !valid_dtype(src_dtype)) return set_error(h, TRL_ENOTSUP, "unsupported dtype");
+  if (count < 0) return set_error(h, TRL_EINVAL, "negative count");
+  if (count == 0) return TRL_OK;
+  if (!dst || !src) return set_error(h, TRL_EINVAL, "null pointer");
+  ProfScope prof(h, PROF_COPY, static_cast<double>(count) * (elt_size(dst_dtype) + elt_size(src_dtype)));
+  if (dst_dtype == src_dtype) return trl_cuda_memcpy(h, dst, src, static_cast<size_t>(count) * elt_size(dst_dtype), TRL_D2D);
+  const unsigned grid = grid_for(h, count, kThreads * 4, 8);
+  if (dst_dtype == TRL_F64)
+    k_convert<double, float><<<grid, kThreads, 0, h->stream>>>(static_cast<double*>(dst), static_cast<const float*>(src), count);
+  else
+    k_convert<float, double><<<grid, kThreads, 0, h->stream>>>(static_cast<float*>(dst), static_cast<const double*>(src), count);
+  return after_launch(h, "convert");
+}
+
+int trl_cuda_bv_mult(trl_cuda_handle h, int dtype, int mode, const void* X, const double* W, void* Y, int64_t n, int bs)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (n == 0) return TRL_OK;
+  if (!X || !W || !Y) return set_error(h, TRL_EINVAL, "null pointer");
+  int transpose = 0, accumulate = 0;
+  double sign = 1.0;
+  switch (mode) {
+  case TRL_MULT: break;
+  case TRL_MULT_TRANSPOSE: transpose = 1; break;
+  case TRL_MULT_ADD: accumulate = 1; break;
+  case TRL_SUBTRACT:
+    accumulate = 1;
+    sign = -1.0;
+    break;
+  default: return set_error(h, TRL_EINVAL, "bad mult mode %d", mode);
+  }
+  if (X == Y && accumulate) return set_error(h, TRL_EINVAL, "accumulating mult requires distinct input and output");
+  ProfScope prof(h, PROF_MULT, (accumulate ? 3.0 : 2.0) * n * bs * elt_size(dtype), 2.0 * n * bs * bs);
+  int st = TRL_OK;
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(X), 1, W, 1, transpose, static_cast<T*>(Y), 1, n, accumulate, sign)));
+  return st;
+}
+
+int trl_cuda_block_dot(trl_cuda_handle h, int dtype, const void* V, int nblk, const void* W, int64_t n, int bs, double* C)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (nblk <= 0) return set_error(h, TRL_EINVAL, "nblk must be positive");
+  if (!C) return set_error(h, TRL_EINVAL, "null pointer");
+  if (n == 0) return trl_cuda_memset_zero(h, C, sizeof(double) * nblk * bs * bs); // empty sum
+  if (!V || !W) return set_error(h, TRL_EINVAL, "null pointer");
+  ProfScope prof(h, PROF_DOT, (nblk + 1.0) * n * bs * elt_size(dtype), 2.0 * nblk * n * bs * bs);
+  int st = TRL_OK;
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_dot<T, BS>(h, static_cast<const T*>(V), nblk, static_cast<const T*>(W), n, C)));
+  return st;
+}
+
+int trl_cuda_block_update(trl_cuda_handle h, int dtype, void* W, const void* V, int nblk, const double* C, int64_t n, int bs)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (nblk <= 0) return set_error(h, TRL_EINVAL, "nblk must be positive");
+  if (n == 0) return TRL_OK;
+  if (!V || !W || !C) return set_error(h, TRL_EINVAL, "null pointer");
+  ProfScope prof(h, PROF_UPDATE, (nblk + 2.0) * n * bs * elt_size(dtype), 2.0 * nblk * n * bs * bs);
+  int st = TRL_OK;
+  // Coef(i, 0) = C + i*bs*bs  ->  ldc = 1
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(V), nblk, C, 1, 0, static_cast<T*>(W), 1, n, 1, -1.0)));
+  return st;
+}
+
+int trl_cuda_block_rotate(trl_cuda_handle h, int dtype, const void* V, int m, const double* Y, int ldy, int k, void* W, int64_t n, int bs)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (m <= 0 || k <= 0 || ldy < k) return set_error(h, TRL_EINVAL, "bad rotation shape m=%d k=%d ldy=%d", m, k, ldy);
+  if (n == 0) return TRL_OK;
+  if (!V || !Y || !W) return set_error(h, TRL_EINVAL, "null pointer");
+  const size_t es = elt_size(dtype);
+  const char* v0 = static_cast<const char*>(V);
+  const char* v1 = v0 + static_cast<size_t>(m) * n * bs * es;
+  const char* w0 = static_cast<const char*>(W);
+  const char* w1 = w0 + static_cast<size_t>(k) * n * bs * es;
+  if (w0 < v1 && v0 < w1) return set_error(h, TRL_EINVAL, "rotation output overlaps its input");
+  ProfScope prof(h, PROF_ROTATE, (static_cast<double>(m) + k) * n * bs * es, 2.0 * n * m * k * bs * bs);
+  int st = TRL_OK;
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(V), m, Y, ldy, 0, static_cast<T*>(W), k, n, 0, 1.0)));
+  return st;
+}
+
+int trl_cuda_cholqr(trl_cuda_handle h, int dtype, void* X, int64_t n, int bs, int passes, double* R)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (passes < 1 || passes > 4) return set_error(h, TRL_EINVAL, "passes must be in [1, 4]");
+  if (!X || !R) return set_error(h, TRL_EINVAL, "null pointer");
+  double* small = static_cast<double*>(small_scratch(h));
+  if (!small) return TRL_ENOMEM;
+  double* G = small;
+  double* Uinv = small + 256;
+  ProfScope prof(h, PROF_CHOLQR, 3.0 * passes * n * bs * elt_size(dtype), 4.0 * passes * n * bs * bs);
+  for (int p = 0; p < passes; ++p) {
+    int st = trl_cuda_block_dot(h, dtype, X, 1, X, n, bs, G);
+    if (st) return st;
+    TRL_DISPATCH_BS(bs, k_chol_factor<BS><<<1, 32, 0, h->stream>>>(G, Uinv, R, p == 0, h->d_status));
+    st = after_launch(h, "cholqr factor");
+    if (st) return st;
+    TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(X), 1, Uinv, 1, 0, static_cast<T*>(X), 1, n, 0, 1.0)));
+    if (st) return st;
+  }
+  return TRL_OK;
+}
+
+} // extern "C"
+
+namespace {
+__global__ void __launch_bounds__(kThreads) k_unblock(const double* __restrict__ X, int64_t n, int bs, int ncols, double* __restrict__ out)
+{
+  const int64_t total = n * ncols;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += stride) {
+    const int64_t r = e / ncols;
+    const int c = static_cast<int>(e % ncols);
+    out[e] = X[static_cast<int64_t>(c / bs) * n * bs + r * bs + (c % bs)];
+  }
+}
+} // namespace
+
+extern "C" int trl_cuda_unblock(trl_cuda_handle h, const double* X, int64_t n, int bs, int ncols, double* out)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!valid_bs(bs) || n < 0 || ncols < 0) return set_error(h, TRL_EINVAL, "bad unblock arguments");
+  if (n == 0 || ncols == 0) return TRL_OK;
+  if (!X || !out) return set_error(h, TRL_EINVAL, "null pointer");
+  ProfScope prof(h, PROF_COPY, 16.0 * n * ncols);
+  k_unblock<<<grid_for(h, n * ncols, kThreads * 4, 8), kThreads, 0, h->stream>>>(X, n, bs, ncols, out);
+  return after_launch(h, "unblock");
+}

@@ -1,0 +1,176 @@
+// Shared internals of libtrl_cuda.so (sm_100a). Not part of the public ABI.
+#pragma once
+
+#include "trl_cuda.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+// Device status word bits (sticky until trl_cuda_synchronize reads and clears them).
+#define TRL_DEV_CHOLESKY 0x1
+#define TRL_DEV_EIGEN 0x2
+#define TRL_DEV_TIMEOUT 0x4
+
+struct trl_cuda_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool owns_stream = false;
+  int* d_status = nullptr;  // device status word
+  void* ws = nullptr;       // growable device workspace
+  double* d_small = nullptr; // 1024 doubles of fixed scratch (Gram / factor blocks)
+  size_t ws_bytes = 0;
+  int* pinned_status = nullptr; // pinned host copy of d_status
+  void* pinned = nullptr;   // small pinned host staging buffer
+  size_t pinned_bytes = 0;
+  void* solver = nullptr;   // cusolverDnHandle_t, created on first use
+  void* syevd_work = nullptr;
+  size_t syevd_work_bytes = 0;
+  uint64_t launches = 0;
+  std::string last_error;
+  // per-kernel-class device timing (trl_cuda_profile_*)
+  bool profiling = false;
+  int prof_depth = 0;
+  struct ProfPending {
+    cudaEvent_t a, b;
+    int cls;
+    double bytes, flops;
+  };
+  std::vector<ProfPending> prof_pending;
+  std::vector<cudaEvent_t> prof_free;
+  trl_kernel_stats prof[TRL_PROF_CLASSES] = {};
+};
+
+namespace trl_detail {
+
+int set_error(trl_cuda_context* h, int status, const char* fmt, ...);
+
+// Ensures at least `bytes` of device workspace; returns nullptr and sets an error on failure.
+void* workspace(trl_cuda_context* h, size_t bytes);
+void* pinned(trl_cuda_context* h, size_t bytes);
+
+inline bool valid_bs(int bs) { return bs == 1 || bs == 2 || bs == 4 || bs == 8 || bs == 16; }
+inline bool valid_dtype(int dt) { return dt == TRL_F64 || dt == TRL_F32; }
+
+// Checks cudaGetLastError after a launch and counts the launch.
+int after_launch(trl_cuda_context* h, const char* what);
+
+// 1024 doubles of per-handle device scratch (Gram / factor blocks); nullptr on failure.
+void* small_scratch(trl_cuda_context* h);
+// Releases the cuSOLVER handle and its workspace.
+void destroy_solver(trl_cuda_context* h);
+
+// Kernel classes of the profiler (index into trl_cuda_context::prof).
+enum ProfClass { PROF_SPMM = 0, PROF_DOT, PROF_UPDATE, PROF_ROTATE, PROF_MULT, PROF_CHOLQR, PROF_SUB, PROF_SMALL_EIGEN, PROF_COPY, PROF_SDDMM, PROF_BLOCK_OPS };
+
+cudaEvent_t prof_event(trl_cuda_context* h);
+// Folds completed timings into the per-class totals (after a stream synchronisation).
+void prof_resolve(trl_cuda_context* h);
+
+// Times one C-ABI call (outermost call only) with a pair of events on the handle's stream
+// and credits it with the call's algorithmic bytes and flops.
+class ProfScope {
+public:
+  ProfScope(trl_cuda_context* h, int cls, double bytes, double flops = 0.0)
+      : h_(h)
+      , cls_(cls)
+      , bytes_(bytes)
+      , flops_(flops)
+  {
+    if (!h_->profiling) return;
+    counted_ = true;
+    if (h_->prof_depth++ != 0) return;
+    active_ = true;
+    a_ = prof_event(h_);
+    b_ = prof_event(h_);
+    cudaEventRecord(a_, h_->stream);
+  }
+  ~ProfScope()
+  {
+    if (!counted_) return;
+    --h_->prof_depth;
+    if (!active_) return;
+    cudaEventRecord(b_, h_->stream);
+    h_->prof_pending.push_back({a_, b_, cls_, bytes_, flops_});
+  }
+  ProfScope(const ProfScope&) = delete;
+  ProfScope& operator=(const ProfScope&) = delete;
+
+private:
+  trl_cuda_context* h_;
+  int cls_;
+  double bytes_, flops_;
+  bool counted_ = false, active_ = false;
+  cudaEvent_t a_{}, b_{};
+};
+
+// Grid sizing: a multiple of the SM count, capped by the work available.
+inline unsigned grid_for(const trl_cuda_context* h, int64_t work_items, int items_per_cta, int ctas_per_sm)
+{
+  int64_t need = (work_items + items_per_cta - 1) / items_per_cta;
+  int64_t cap = static_cast<int64_t>(h->num_sms) * ctas_per_sm;
+  if (need < 1) need = 1;
+  return static_cast<unsigned>(need < cap ? need : cap);
+}
+
+} // namespace trl_detail
+
+// FP64 tensor-core MMA, m8n8k4 (DMMA). Fragment layout (PTX ISA, mma.m8n8k4 .f64):
+// with g = lane>>2 and t = lane&3: a = A[g][t], b = B[t][g], {d0,d1} = D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n" : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+template <typename T>
+__device__ __forceinline__ double ld_widen(const T* p)
+{
+  return static_cast<double>(__ldg(p));
+}
+
+#define TRL_CHECK_HANDLE(h)                                                                                                                                                                            \
+  do {                                                                                                                                                                                                 \
+    if (!(h)) return TRL_EINVAL;                                                                                                                                                                       \
+  } while (0)
+
+// Dispatch a block size to a compile-time constant BS.
+#define TRL_DISPATCH_BS(bs, ...)                                                                                                                                                                       \
+  switch (bs) {                                                                                                                                                                                        \
+  case 1: {                                                                                                                                                                                            \
+    constexpr int BS = 1;                                                                                                                                                                              \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  } break;                                                                                                                                                                                             \
+  case 2: {                                                                                                                                                                                            \
+    constexpr int BS = 2;                                                                                                                                                                              \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  } break;                                                                                                                                                                                             \
+  case 4: {                                                                                                                                                                                            \
+    constexpr int BS = 4;                                                                                                                                                                              \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  } break;                                                                                                                                                                                             \
+  case 8: {                                                                                                                                                                                            \
+    constexpr int BS = 8;                                                                                                                                                                              \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  } break;                                                                                                                                                                                             \
+  case 16: {                                                                                                                                                                                           \
+    constexpr int BS = 16;                                                                                                                                                                             \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  } break;                                                                                                                                                                                             \
+  default: return trl_detail::set_error(h, TRL_ENOTSUP, "unsupported block size %d", bs);                                                                                                             \
+  }
+
+#define TRL_DISPATCH_DT(dt, ...)                                                                                                                                                                       \
+  if ((dt) == TRL_F64) {                                                                                                                                                                               \
+    using T = double;                                                                                                                                                                                  \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  }                                                                                                                                                                                                    \
+  else if ((dt) == TRL_F32) {                                                                                                                                                                          \
+    using T = float;                                                                                                                                                                                   \
+    __VA_ARGS__;                                                                                                                                                                                       \
+  }                                                                                                                                                                                                    \
+  else                                                                                                                                                                                                 \
+    return trl_detail::set_error(h, TRL_ENOTSUP, "unsupported dtype %d", dt);

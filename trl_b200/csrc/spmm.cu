@@ -1,0 +1,255 @@
+// CSR sparse operator against a row-major block: Y = alpha*A*X + beta*X, and the SDDMM
+// used by the eigenvalue adjoint.
+//
+// SpMM scheduling: a row is owned by a group of LPR lanes; each lane carries VEC adjacent
+// columns of the block so that one X row is gathered with LPR 16-byte loads. The group
+// reads LPR consecutive (col, val) pairs with one coalesced load per lane and broadcasts
+// them with group-local shuffles, so every X gather is issued without waiting on index
+// loads of the other entries. Accumulation is in the storage type (FP32 for the mixed
+// mode, as the FP32 SpMM is specified; FP64 otherwise).
+#include "common.cuh"
+
+#include <cstring>
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename T, int VEC>
+struct VecT;
+template <>
+struct VecT<double, 1> {
+  using type = double;
+};
+template <>
+struct VecT<double, 2> {
+  using type = double2;
+};
+template <>
+struct VecT<float, 1> {
+  using type = float;
+};
+template <>
+struct VecT<float, 2> {
+  using type = float2;
+};
+template <>
+struct VecT<float, 4> {
+  using type = float4;
+};
+
+template <typename T, int VEC>
+__device__ __forceinline__ void load_vec(const T* p, T (&out)[VEC])
+{
+  using V = typename VecT<T, VEC>::type;
+  const V v = __ldg(reinterpret_cast<const V*>(p));
+  if constexpr (VEC == 1) {
+    out[0] = reinterpret_cast<const T*>(&v)[0];
+  }
+  else {
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) out[i] = reinterpret_cast<const T*>(&v)[i];
+  }
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void store_vec(T* p, const T (&in)[VEC])
+{
+  using V = typename VecT<T, VEC>::type;
+  V v;
+#pragma unroll
+  for (int i = 0; i < VEC; ++i) reinterpret_cast<T*>(&v)[i] = in[i];
+  *reinterpret_cast<V*>(p) = v;
+}
+
+template <typename T, int BS>
+struct SpmmShape {
+  static constexpr int max_vec = 16 / static_cast<int>(sizeof(T));
+  static constexpr int VEC = max_vec < BS ? max_vec : BS;
+  static constexpr int LPR = BS / VEC;                // lanes per row: 1..8
+  static constexpr int RPW = 32 / LPR;                // rows per warp
+  static constexpr int UR = LPR >= 8 ? 1 : 8 / LPR;   // index rounds per iteration: 8 entries
+};
+
+template <typename T, int BS>
+__global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const T* __restrict__ vals,
+                                                   const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta)
+{
+  using S = SpmmShape<T, BS>;
+  constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UR = S::UR;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % LPR;
+  const int grp = lane / LPR;
+  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (grp * LPR));
+  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
+  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
+
+  for (int64_t rbase = warp_global * RPW; rbase < n; rbase += warp_stride * RPW) {
+    const int64_t row = rbase + grp;
+    if (row >= n) continue; // uniform within the lane group
+    const int kbeg = __ldg(rowptr + row);
+    const int kend = __ldg(rowptr + row + 1);
+    T acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = T(0);
+    for (int k = kbeg; k < kend; k += LPR * UR) {
+      // UR rounds of LPR (col, val) pairs: one coalesced load per lane per round ...
+      int c[UR];
+      T v[UR];
+#pragma unroll
+      for (int u = 0; u < UR; ++u) {
+        const int kk = k + u * LPR + sub;
+        c[u] = 0;
+        v[u] = T(0);
+        if (kk < kend) {
+          c[u] = __ldg(colind + kk);
+          v[u] = __ldg(vals + kk);
+        }
+      }
+      // ... then every X gather of the iteration before the first FMA
+      T x[UR][LPR][VEC];
+#pragma unroll
+      for (int u = 0; u < UR; ++u)
+#pragma unroll
+        for (int t = 0; t < LPR; ++t) {
+          const int ct = (LPR == 1) ? c[u] : __shfl_sync(gmask, c[u], t, LPR);
+          if (k + u * LPR + t < kend) {
+            load_vec<T, VEC>(X + static_cast<int64_t>(ct) * BS + sub * VEC, x[u][t]);
+          }
+          else {
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) x[u][t][i] = T(0);
+          }
+        }
+#pragma unroll
+      for (int u = 0; u < UR; ++u)
+#pragma unroll
+        for (int t = 0; t < LPR; ++t) {
+          const T wt = (LPR == 1) ? v[u] : __shfl_sync(gmask, v[u], t, LPR);
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) acc[i] = fma(wt, x[u][t][i], acc[i]);
+        }
+    }
+    T y[VEC];
+    if (beta != T(0)) {
+      T x[VEC];
+      load_vec<T, VEC>(X + row * BS + sub * VEC, x);
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i] + beta * x[i];
+    }
+    else {
+#pragma unroll
+      for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i];
+    }
+    store_vec<T, VEC>(Y + row * BS + sub * VEC, y);
+  }
+}
+
+// out[p] = sum_c w[c] X[row(p), c] X[col(p), c]; one warp per row, lanes over its entries.
+__global__ void __launch_bounds__(kThreads) k_sddmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const double* __restrict__ X, int k,
+                                                    const double* __restrict__ w, double* __restrict__ out)
+{
+  const int lane = threadIdx.x & 31;
+  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
+  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
+  for (int64_t row = warp_global; row < n; row += warp_stride) {
+    const int kbeg = __ldg(rowptr + row), kend = __ldg(rowptr + row + 1);
+    const double* xr = X + row * k;
+    for (int p = kbeg + lane; p < kend; p += 32) {
+      const double* xc = X + static_cast<int64_t>(__ldg(colind + p)) * k;
+      double s = 0.0;
+      for (int c = 0; c < k; ++c) s = fma(__ldg(w + c) * __ldg(xr + c), __ldg(xc + c), s);
+      out[p] = s;
+    }
+  }
+}
+
+} // namespace
+
+using namespace trl_detail;
+
+extern "C" {
+
+int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!A || !X || !Y) return set_error(h, TRL_EINVAL, "null pointer");
+  if (!valid_dtype(dtype) || A->value_dtype != dtype) return set_error(h, TRL_ENOTSUP, "SpMM needs CSR values and block in the same dtype (got %d and %d)", A->value_dtype, dtype);
+  if (!valid_bs(bs)) return set_error(h, TRL_ENOTSUP, "unsupported block size %d", bs);
+  if (A->n < 0 || A->nnz < 0 || A->nnz >= (int64_t(1) << 31)) return set_error(h, TRL_EINVAL, "bad CSR sizes");
+  if (A->n == 0) return TRL_OK;
+  if (!A->rowptr || (A->nnz > 0 && (!A->colind || !A->values))) return set_error(h, TRL_EINVAL, "null CSR array");
+  if (X == Y) return set_error(h, TRL_EINVAL, "SpMM input and output must not alias");
+  const size_t es = dtype == TRL_F64 ? 8 : 4;
+  if (((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) % (es * bs < 16 ? es * bs : 16)) != 0)
+    return set_error(h, TRL_EINVAL, "block vectors must be aligned to min(16, bs*elem) bytes");
+  ProfScope prof(h, PROF_SPMM, A->nnz * (es + 4.0) + 4.0 * (A->n + 1) + 2.0 * A->n * bs * es, 2.0 * A->nnz * bs);
+  int st = TRL_OK;
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
+    using S = SpmmShape<T, BS>;
+    const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, 16);
+    k_spmm<T, BS><<<grid, kThreads, 0, h->stream>>>(A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
+                                                    static_cast<T>(alpha), static_cast<T>(beta));
+    st = after_launch(h, "spmm");
+  }));
+  return st;
+}
+
+int trl_cuda_sddmm(trl_cuda_handle h, const trl_csr* P, const double* X, int k, const double* w, double* out)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!P || !X || !w || !out) return set_error(h, TRL_EINVAL, "null pointer");
+  if (k <= 0) return set_error(h, TRL_EINVAL, "k must be positive");
+  if (P->n == 0 || P->nnz == 0) return TRL_OK;
+  ProfScope prof(h, PROF_SDDMM, 12.0 * P->nnz + 4.0 * (P->n + 1) + 8.0 * P->n * k, 3.0 * P->nnz * k);
+  const unsigned grid = grid_for(h, P->n, kThreads / 32, 16);
+  k_sddmm<<<grid, kThreads, 0, h->stream>>>(P->n, P->rowptr, P->colind, X, k, w, out);
+  return after_launch(h, "sddmm");
+}
+
+} // extern "C"
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_norm1(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const void* __restrict__ vals, int f64,
+                                               double alpha, double beta, unsigned long long* __restrict__ out)
+{
+  double best = 0.0;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    bool diag = false;
+    for (int p = rowptr[r]; p < rowptr[r + 1]; ++p) {
+      const double a = f64 ? static_cast<const double*>(vals)[p] : static_cast<double>(static_cast<const float*>(vals)[p]);
+      if (colind[p] == r) {
+        s += fabs(alpha * a + beta);
+        diag = true;
+      }
+      else
+        s += fabs(alpha * a);
+    }
+    if (!diag) s += fabs(beta);
+    best = fmax(best, s);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+  // non-negative doubles order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(best)));
+}
+
+} // namespace
+
+extern "C" int trl_cuda_csr_norm1(trl_cuda_handle h, const trl_csr* A, double alpha, double beta, double* host_out)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!A || !host_out) return set_error(h, TRL_EINVAL, "null pointer");
+  *host_out = 0.0;
+  if (A->n == 0) return TRL_OK;
+  unsigned long long* d = static_cast<unsigned long long*>(workspace(h, 64));
+  if (!d) return TRL_ENOMEM;
+  cudaMemsetAsync(d, 0, sizeof(unsigned long long), h->stream);
+  k_norm1<<<grid_for(h, A->n, 256, 8), 256, 0, h->stream>>>(A->n, A->rowptr, A->colind, A->values, A->value_dtype == TRL_F64, alpha, beta, d);
+  if (int st = after_launch(h, "csr_norm1")) return st;
+  unsigned long long bits = 0;
+  if (int st = trl_cuda_memcpy(h, &bits, d, sizeof bits, TRL_D2H)) return st;
+  std::memcpy(host_out, &bits, sizeof bits);
+  return TRL_OK;
+}
