@@ -134,6 +134,27 @@ int trl_cuda_unblock(trl_cuda_handle h, const double* X, int64_t n, int bs, int 
  * reduction (the result does not depend on scheduling). */
 int trl_cuda_block_dot(trl_cuda_handle h, int dtype, const void* V, int nblk, const void* W, int64_t n, int bs, double* C);
 
+/* Allocation-free variant of trl_cuda_block_dot. It has no counterpart in the reference.
+ *
+ * For callers that may not allocate device memory: programs that hand all GPU memory to
+ * their own pool allocator and do not let libraries call cudaMalloc behind their back, and
+ * latency-critical loops that cannot afford an allocation or the device-wide
+ * synchronisation that freeing one brings. It needs no handle either (creating a handle
+ * allocates): pass the cudaStream_t to enqueue on and make the stream's device current.
+ *
+ * Computes the same C_j = V_j^T W (j < nblk) as trl_cuda_block_dot. Its partial sums go to
+ * a fixed array inside this library (2 MiB of device memory on every GPU that loads the
+ * library, held until the process exits), so nblk*bs*bs may be at most
+ * TRL_CUDA_NOALLOC_MAX_ENTRIES; larger requests return TRL_EINVAL and do nothing.
+ * The first call on each device looks up that array's device address (once per device, with
+ * the device current); make that first call before any stream capture. All calls share the
+ * one array: calls that may run at the same time on the GPU (different streams, or several
+ * threads) race on it and must be serialised by the caller. The array's contents left by a
+ * previous call are never read.
+ * Returns TRL_OK, TRL_EINVAL, TRL_ENOTSUP or TRL_ECUDA (no error message is recorded). */
+#define TRL_CUDA_NOALLOC_MAX_ENTRIES 16384
+int trl_cuda_block_dot_noalloc(void* stream, int dtype, const void* V, int nblk, const void* W, int64_t n, int bs, double* C);
+
 /* Projection update W -= sum_{j<nblk} V_j C_j (C as returned by trl_cuda_block_dot).
  * With trl_cuda_block_dot this is one classical Gram-Schmidt pass against nblk blocks,
  * replacing nblk rounds of ModifiedGS (reorthogonalization.hh:14-21). */

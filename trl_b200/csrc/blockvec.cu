@@ -614,3 +614,97 @@ extern "C" int trl_cuda_unblock(trl_cuda_handle h, const double* X, int64_t n, i
   k_unblock<<<grid_for(h, n * ncols, kThreads * 4, 8), kThreads, 0, h->stream>>>(X, n, bs, ncols, out);
   return after_launch(h, "unblock");
 }
+
+// ---------------------------------------------------------------- allocation-free block dot
+// trl_cuda_block_dot_noalloc: the multi-block inner product for callers that must not
+// allocate device memory. Its per-chunk partial sums live in the fixed array below instead
+// of a handle's workspace. One copy of the array (2 MiB) exists on every GPU that loads this
+// library and stays there until the process exits.
+#include <mutex>
+
+static constexpr int64_t kNoAllocScratchDoubles = int64_t(1) << 18; // 2 MiB of FP64 partials
+static constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocScratchDoubles];
+
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+static int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// Resolves the device address of the scratch array on the current device (once per device).
+static int noalloc_scratch(int device, double** ptr, int* sms)
+{
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return TRL_ECUDA;
+    }
+    int count = 0;
+    if (cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || count <= 0) {
+      cudaGetLastError();
+      return TRL_ECUDA;
+    }
+    g_noalloc_sms[device] = count;
+    g_noalloc_ptr[device] = static_cast<double*>(p);
+  }
+  *ptr = g_noalloc_ptr[device];
+  *sms = g_noalloc_sms[device];
+  return TRL_OK;
+}
+
+template <typename T, int BS, int JC, int G>
+static int noalloc_dot(cudaStream_t stream, int sms, double* partial, const T* V, int nblk, const T* W, int64_t n, double* C)
+{
+  const int64_t len = static_cast<int64_t>(nblk) * BS * BS;
+  const int gj = (nblk + JC - 1) / JC;
+  int64_t chunks = static_cast<int64_t>(sms) * 4 / gj;
+  const int64_t fit = kNoAllocScratchDoubles / len; // chunks whose partials fit the array
+  if (chunks > fit) chunks = fit;
+  const int64_t max_chunks = (n + 511) / 512;
+  if (chunks > max_chunks) chunks = max_chunks;
+  if (chunks < 1) chunks = 1;
+  int64_t rows_per_cta = (n + chunks - 1) / chunks;
+  constexpr int step = kWarps * 4 * G;
+  rows_per_cta = (rows_per_cta + step - 1) / step * step;
+  chunks = (n + rows_per_cta - 1) / rows_per_cta;
+  // every (chunk, block) entry of the partials is written before it is read in this call,
+  // so nothing left in the array by an earlier call is used and nothing needs clearing
+  k_block_dot<T, BS, JC, G><<<dim3(gj, static_cast<unsigned>(chunks)), kThreads, 0, stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial);
+  if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, stream>>>(partial, static_cast<int>(chunks), len, C);
+  if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
+  return TRL_OK;
+}
+
+template <typename T, int BS>
+static int noalloc_dot_dispatch(cudaStream_t stream, int sms, double* partial, const T* V, int nblk, const T* W, int64_t n, double* C)
+{
+  if (nblk == 1) return noalloc_dot<T, BS, 1, 8>(stream, sms, partial, V, nblk, W, n, C);
+  if (nblk == 2) return noalloc_dot<T, BS, 2, 4>(stream, sms, partial, V, nblk, W, n, C);
+  if (nblk <= 4) return noalloc_dot<T, BS, 4, (BS >= 16 ? 2 : 4)>(stream, sms, partial, V, nblk, W, n, C);
+  return noalloc_dot<T, BS, (BS >= 16 ? 4 : 8), 2>(stream, sms, partial, V, nblk, W, n, C);
+}
+
+extern "C" int trl_cuda_block_dot_noalloc(void* stream, int dtype, const void* V, int nblk, const void* W, int64_t n, int bs, double* C)
+{
+  if (!valid_dtype(dtype) || !valid_bs(bs)) return TRL_ENOTSUP;
+  if (nblk <= 0 || n < 0 || !C) return TRL_EINVAL;
+  if (static_cast<int64_t>(nblk) * bs * bs > TRL_CUDA_NOALLOC_MAX_ENTRIES) return TRL_EINVAL; // the output would not fit the partial-sum array
+  auto s = static_cast<cudaStream_t>(stream);
+  if (n == 0) return cudaMemsetAsync(C, 0, sizeof(double) * nblk * bs * bs, s) == cudaSuccess ? TRL_OK : TRL_ECUDA;
+  if (!V || !W) return TRL_EINVAL;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kNoAllocMaxDevices) {
+    cudaGetLastError();
+    return TRL_ECUDA;
+  }
+  double* partial = nullptr;
+  int sms = 0;
+  if (int st = noalloc_scratch(device, &partial, &sms)) return st;
+  int st = TRL_OK;
+  trl_cuda_context* h = nullptr; // only for the dispatch macros' error path
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = noalloc_dot_dispatch<T, BS>(s, sms, partial, static_cast<const T*>(V), nblk, static_cast<const T*>(W), n, C)));
+  return st;
+}

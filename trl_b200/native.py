@@ -48,6 +48,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_convert": (C.c_int, [P, C.c_int, P, C.c_int, P, I64]),
     "trl_cuda_unblock": (C.c_int, [P, P, I64, C.c_int, C.c_int, P]),
     "trl_cuda_block_dot": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, P]),
+    "trl_cuda_block_dot_noalloc": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, P]),
     "trl_cuda_block_update": (C.c_int, [P, C.c_int, P, P, C.c_int, P, I64, C.c_int]),
     "trl_cuda_block_rotate": (C.c_int, [P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, P, I64, C.c_int]),
     "trl_cuda_cholqr": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P]),
