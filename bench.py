@@ -238,7 +238,7 @@ def trl_arm(args, world, rank, local):
     for name, s in prof.items():
         if s["calls"] == 0:
             continue
-        kern[name] = {"calls": s["calls"], "seconds": s["seconds"], "share": None,
+        kern[name] = {"calls": s["calls"], "seconds": s["seconds"], "share": None, "bytes_per_call": s["bytes"] / s["calls"],
                       "gbs": s["bytes"] / s["seconds"] / 1e9 if s["seconds"] > 0 else None,
                       "tflops": s["flops"] / s["seconds"] / 1e12 if s["seconds"] > 0 else None}
     tot = sum(v["seconds"] for v in kern.values())
@@ -246,9 +246,12 @@ def trl_arm(args, world, rank, local):
         v["share"] = v["seconds"] / tot if tot else None
     dominant = max(kern, key=lambda k: kern[k]["seconds"])
     d = kern[dominant]
-    traffic = load_traffic(dominant)
-    roofline = {"kernel": dominant, "bound": "hbm", "achieved": d["gbs"], "peak": hbm, "unit": "GB/s", "frac": d["gbs"] / hbm,
-                "traffic": traffic, "peak_source": src}
+    # achieved = algorithmic bytes per call / mean call duration (CUDA events on the solver's
+    # stream around every call of the class during the timed solves)
+    achieved = d["bytes_per_call"] / (d["seconds"] / d["calls"]) / 1e9
+    traffic = load_traffic(dominant, d["bytes_per_call"])
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": traffic, "algorithmic_bytes_per_call": d["bytes_per_call"], "peak_source": src}
     spmm = kern.get("spmm", {})
 
     result = None
@@ -289,12 +292,14 @@ def trl_arm(args, world, rank, local):
     return result
 
 
-def load_traffic(kernel: str):
-    """DRAM bytes per call from the committed ncu summary of that kernel, if present."""
+def load_traffic(kernel: str, algorithmic_bytes_per_call: float):
+    """DRAM bytes per call: the committed ncu ratio (DRAM traffic / algorithmic bytes, from a
+    capture of the same kernel on a smaller case) times this run's algorithmic bytes per call."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(kernel)
+            r = json.load(f).get(kernel)
+        return None if r is None else r["traffic_per_algorithmic"] * algorithmic_bytes_per_call
     except Exception:
         return None
 
@@ -317,6 +322,54 @@ def cpu_baseline(A, X0, restarts_gpu: int):
                       f"(the reference's restart count for this workload)"}
 
 
+def profile_case(args):
+    """Runs one piece of the workload, without timing output, for profiler captures:
+    solve   one FP64 solve capped at --restarts restart cycles (launch lists);
+    spmm    the operator apply on the full workload (CSR 113 MB, X and Y 57 MB each);
+    dot / update   one multi-block inner product / projection update against --nblk
+            basis blocks of the workload (n x 8 FP64 each);
+    rotate  the thick-restart rotation V (48 blocks) x Y -> 5 blocks.
+    Every case reads and writes more than the 126 MB L2 and holds at most ~3 GB."""
+    import torch
+
+    from trl_b200 import native
+    from trl_b200 import problems as P
+
+    bs = CFG["bs"]
+    dt = torch.float32 if args.fp32 else torch.float64
+    A = P.anisotropic3d(CFG["grid"], coef=CFG["coef"])
+    h = native.Handle(0)
+    if args.case == "solve":
+        A64 = native.DeviceCSRTensors.from_host(A)
+        A32 = native.DeviceCSRTensors.from_host(A, torch.float32)
+        X0 = torch.from_numpy(P.initial_block(A.n, bs, seed=CFG["seed"])).cuda()
+        mode = native.TRL_MODE_FP32 if args.fp32 else native.TRL_MODE_FP64
+        native.solve_csr_device(h, A64, A32, X0, bs=bs, nev=CFG["nev"], ncv=CFG["ncv"], tol=CFG["tol"], mode=mode, max_restarts=args.restarts, want_vectors=0)
+    elif args.case == "spmm":
+        Ad = native.DeviceCSRTensors.from_host(A, dt)
+        X = torch.randn(A.n, bs, dtype=dt, device="cuda")
+        Y = torch.empty_like(X)
+        for _ in range(args.reps):
+            h.spmm(Ad, X, Y)
+    elif args.case in ("dot", "update"):
+        V = torch.randn(args.nblk, A.n, bs, dtype=dt, device="cuda")
+        w = torch.randn(A.n, bs, dtype=dt, device="cuda")
+        Cm = torch.randn(args.nblk, bs, bs, dtype=torch.float64, device="cuda") * 1e-3
+        for _ in range(args.reps):
+            if args.case == "dot":
+                h.block_dot(V, w, Cm)
+            else:
+                h.block_update(w, V, Cm)
+    elif args.case == "rotate":
+        V = torch.randn(48, A.n, bs, dtype=dt, device="cuda")
+        Y = torch.randn(48, 48, bs, bs, dtype=torch.float64, device="cuda")
+        W = torch.empty(5, A.n, bs, dtype=dt, device="cuda")
+        for _ in range(args.reps):
+            h.block_rotate(V, Y, 5, W)
+    torch.cuda.synchronize()
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -325,7 +378,16 @@ def main():
     ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
     ap.add_argument("--fp32-tol", type=float, default=1e-5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["solve", "spmm", "dot", "update", "rotate"], default=None,
+                    help="profiling driver: run one piece of the workload and exit (see profile_case)")
+    ap.add_argument("--restarts", type=int, default=3)
+    ap.add_argument("--nblk", type=int, default=24)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--fp32", action="store_true")
     args = ap.parse_args()
+    if args.case:
+        profile_case(args)
+        return
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         reference_arm(args, world, rank)

@@ -66,82 +66,104 @@ template <typename T, int BS>
 struct SpmmShape {
   static constexpr int max_vec = 16 / static_cast<int>(sizeof(T));
   static constexpr int VEC = max_vec < BS ? max_vec : BS;
-  static constexpr int LPR = BS / VEC;                // lanes per row: 1..8
-  static constexpr int RPW = 32 / LPR;                // rows per warp
-  static constexpr int UR = LPR >= 8 ? 1 : 8 / LPR;   // index rounds per iteration: 8 entries
+  static constexpr int LPR = BS / VEC;              // lanes per row: 1..8
+  static constexpr int RPW = 32 / LPR;              // rows per warp iteration
+  static constexpr int UG = VEC >= 4 ? 4 : 8;       // gathers a lane issues before its FMAs
+  static constexpr int CH = 64;                     // (col, val) pairs staged per warp per chunk
 };
 
+// A warp owns RPW consecutive rows per iteration; within it a group of LPR lanes owns a row
+// and each lane VEC adjacent columns of the block.
+//  1. rowptr of the warp's rows is loaded one iteration ahead (software prefetch);
+//  2. the rows' (col, val) pairs - one contiguous CSR range - are staged in shared memory
+//     with coalesced warp-wide loads, CH pairs at a time;
+//  3. each group walks its row's pairs in the stage and issues UG independent 16-byte X
+//     gathers before the FMAs that consume them.
 template <typename T, int BS>
 __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const T* __restrict__ vals,
                                                    const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta)
 {
   using S = SpmmShape<T, BS>;
-  constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UR = S::UR;
-  const int lane = threadIdx.x & 31;
+  constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH;
+  constexpr int WPC = kThreads / 32;
+  __shared__ int s_col[WPC][CH];
+  __shared__ T s_val[WPC][CH];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int sub = lane % LPR;
   const int grp = lane / LPR;
-  const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (grp * LPR));
-  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
-  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
+  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * WPC + w;
+  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * WPC;
+  int64_t rbase = warp_global * RPW;
+  if (rbase >= n) return; // whole warp
+  // lane l < RPW holds rowptr[row l], every lane holds the end offset rowptr[row RPW]
+  // (rows past n read rowptr[n]: empty rows)
+  int rp = (lane < RPW) ? __ldg(rowptr + min(rbase + lane, n)) : 0;
+  int rpe = __ldg(rowptr + min(rbase + RPW, n));
 
-  for (int64_t rbase = warp_global * RPW; rbase < n; rbase += warp_stride * RPW) {
-    const int64_t row = rbase + grp;
-    if (row >= n) continue; // uniform within the lane group
-    const int kbeg = __ldg(rowptr + row);
-    const int kend = __ldg(rowptr + row + 1);
+  for (; rbase < n; rbase += warp_stride * RPW) {
+    const int64_t nbase = rbase + warp_stride * RPW;
+    const int rp_next = (nbase < n && lane < RPW) ? __ldg(rowptr + min(nbase + lane, n)) : 0;
+    const int rpe_next = (nbase < n) ? __ldg(rowptr + min(nbase + RPW, n)) : 0;
+    const int s = __shfl_sync(0xffffffffu, rp, 0);
+    const int e = rpe;
+    const int kb = __shfl_sync(0xffffffffu, rp, grp);
+    const int kn = __shfl_sync(0xffffffffu, rp, (grp + 1) & 31);
+    const int ke = (grp + 1 == RPW) ? rpe : kn;
     T acc[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) acc[i] = T(0);
-    for (int k = kbeg; k < kend; k += LPR * UR) {
-      // UR rounds of LPR (col, val) pairs: one coalesced load per lane per round ...
-      int c[UR];
-      T v[UR];
+
+    for (int cs = s; cs < e; cs += CH) { // uniform over the warp
 #pragma unroll
-      for (int u = 0; u < UR; ++u) {
-        const int kk = k + u * LPR + sub;
-        c[u] = 0;
-        v[u] = T(0);
-        if (kk < kend) {
-          c[u] = __ldg(colind + kk);
-          v[u] = __ldg(vals + kk);
+      for (int q = 0; q < CH / 32; ++q) {
+        const int p = cs + q * 32 + lane;
+        if (p < e) {
+          s_col[w][q * 32 + lane] = __ldg(colind + p);
+          s_val[w][q * 32 + lane] = __ldg(vals + p);
         }
       }
-      // ... then every X gather of the iteration before the first FMA
-      T x[UR][LPR][VEC];
+      __syncwarp();
+      const int lo = max(kb, cs) - cs, hi = min(ke, cs + CH) - cs;
+      for (int t = lo; t < hi; t += UG) {
+        T x[UG][VEC];
+        T wv[UG];
 #pragma unroll
-      for (int u = 0; u < UR; ++u)
-#pragma unroll
-        for (int t = 0; t < LPR; ++t) {
-          const int ct = (LPR == 1) ? c[u] : __shfl_sync(gmask, c[u], t, LPR);
-          if (k + u * LPR + t < kend) {
-            load_vec<T, VEC>(X + static_cast<int64_t>(ct) * BS + sub * VEC, x[u][t]);
+        for (int u = 0; u < UG; ++u) {
+          if (t + u < hi) {
+            wv[u] = s_val[w][t + u];
+            load_vec<T, VEC>(X + static_cast<int64_t>(s_col[w][t + u]) * BS + sub * VEC, x[u]);
           }
           else {
+            wv[u] = T(0);
 #pragma unroll
-            for (int i = 0; i < VEC; ++i) x[u][t][i] = T(0);
+            for (int i = 0; i < VEC; ++i) x[u][i] = T(0);
           }
         }
 #pragma unroll
-      for (int u = 0; u < UR; ++u)
+        for (int u = 0; u < UG; ++u)
 #pragma unroll
-        for (int t = 0; t < LPR; ++t) {
-          const T wt = (LPR == 1) ? v[u] : __shfl_sync(gmask, v[u], t, LPR);
-#pragma unroll
-          for (int i = 0; i < VEC; ++i) acc[i] = fma(wt, x[u][t][i], acc[i]);
-        }
+          for (int i = 0; i < VEC; ++i) acc[i] = fma(wv[u], x[u][i], acc[i]);
+      }
+      __syncwarp();
     }
-    T y[VEC];
-    if (beta != T(0)) {
-      T x[VEC];
-      load_vec<T, VEC>(X + row * BS + sub * VEC, x);
+
+    const int64_t row = rbase + grp;
+    if (row < n) {
+      T y[VEC];
+      if (beta != T(0)) {
+        T x[VEC];
+        load_vec<T, VEC>(X + row * BS + sub * VEC, x);
 #pragma unroll
-      for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i] + beta * x[i];
-    }
-    else {
+        for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i] + beta * x[i];
+      }
+      else {
 #pragma unroll
-      for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i];
+        for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i];
+      }
+      store_vec<T, VEC>(Y + row * BS + sub * VEC, y);
     }
-    store_vec<T, VEC>(Y + row * BS + sub * VEC, y);
+    rp = rp_next;
+    rpe = rpe_next;
   }
 }
 
@@ -187,7 +209,13 @@ int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X,
   int st = TRL_OK;
   TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
     using S = SpmmShape<T, BS>;
-    const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, 16);
+    // one resident wave: every warp strides over the rows (its rowptr prefetch pays off)
+    static int resident = 0;
+    if (resident == 0) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_spmm<T, BS>, kThreads, 0) != cudaSuccess || resident < 1) resident = 4;
+      cudaGetLastError();
+    }
+    const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, resident);
     k_spmm<T, BS><<<grid, kThreads, 0, h->stream>>>(A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
                                                     static_cast<T>(alpha), static_cast<T>(beta));
     st = after_launch(h, "spmm");
