@@ -265,7 +265,8 @@ def trl_arm(args, world, rank, local):
             "metric": METRIC, "value": ms64 / 1e3, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms64, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "mode": "fp64", "reorth": "block CGS2", "orthonormalize": "CholQR2",
+            "config": {"workload": WORKLOAD, "mode": "fp64", "reorth": "block classical Gram-Schmidt, second pass if needed (DGKS)",
+                       "orthonormalize": "CholQR2",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (basis 2.8 GB, CSR 113 MB, per-step working set >> 126 MB)"},
             "fp64": {"seconds": ms64 / 1e3, "restarts": o64["restarts"], "n_op_apply": o64["n_op_apply"], "converged": bool(o64["converged"]),

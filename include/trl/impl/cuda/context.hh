@@ -128,9 +128,15 @@ public:
     push({1, dtype, bs, n, in, coef, out});
   }
 
+  /// Operation sequence number: advances with every backend operation (each one flushes or
+  /// records). Lets a result computed by one operation be reused by the next one only if
+  /// nothing ran in between.
+  std::uint64_t seq() const { return seq_; }
+
   /// Executes every recorded operation (fused when the pattern allows).
   void flush()
   {
+    ++seq_;
     if (pending_.empty()) return;
     std::vector<Op> ops;
     ops.swap(pending_);
@@ -150,9 +156,11 @@ private:
   bool batching_ = true;
   std::vector<Op> pending_;
   std::uint64_t fused_ = 0;
+  std::uint64_t seq_ = 0;
 
   void push(const Op& op)
   {
+    ++seq_;
     if (!pending_.empty()) {
       const Op& f = pending_.front();
       if (f.dtype != op.dtype || f.bs != op.bs || f.n != op.n) flush();

@@ -54,8 +54,13 @@ public:
 
   virtual void orthonormalize(BlockView V, BlockMatrixBlockView R)
   {
+    // The Gram matrix V^T V is reused when the reorthogonalisation that just ran on this
+    // very block formed it (and no other operation ran since).
+    const bool reuse = gram_block_ == V.data_ && gram_seq_ == ctx_->seq();
+    gram_block_ = nullptr;
     ctx_->flush();
-    ctx_->check(trl_cuda_cholqr(ctx_->handle(), dtype, V.data_, static_cast<std::int64_t>(N), blocksize, cholqr_passes_, R.data_), "orthonormalize");
+    const double* G0 = reuse ? static_cast<const double*>(gram_.get()) : nullptr;
+    ctx_->check(trl_cuda_cholqr_gram(ctx_->handle(), dtype, V.data_, static_cast<std::int64_t>(N), blocksize, cholqr_passes_, R.data_, G0), "orthonormalize");
   }
 
   std::size_t size() const { return N; }
@@ -100,19 +105,19 @@ public:
   void set_cholqr_passes(int p) { cholqr_passes_ = p; }
   int cholqr_passes() const { return cholqr_passes_; }
 
-  /// w <- w - V[0:count] (V[0:count]^T w), repeated `passes` times (classical Gram-Schmidt
-  /// against `count` contiguous blocks starting at V0).
-  void project_out(BlockView V0, unsigned int count, BlockView w, int passes)
+  /// Classical Gram-Schmidt of w against the `count` contiguous blocks starting at V0
+  /// (trl_cuda_project_out; mode TRL_CGS_ONE / TRL_CGS_TWO / TRL_CGS_IFNEEDED). Keeps the
+  /// Gram matrix of the result for the orthonormalize() that follows.
+  void project_out(BlockView V0, unsigned int count, BlockView w, int mode, double eta = 0.70710678118654752)
   {
     if (count == 0) return;
     ctx_->flush();
-    const std::size_t need = sizeof(double) * count * blocksize * blocksize;
-    if (coef_.bytes() < need) coef_ = DeviceBuffer(ctx_, need);
-    auto* C = static_cast<double*>(coef_.get());
-    for (int p = 0; p < passes; ++p) {
-      ctx_->check(trl_cuda_block_dot(ctx_->handle(), dtype, V0.data_, static_cast<int>(count), w.data_, static_cast<std::int64_t>(N), blocksize, C), "project_out dot");
-      ctx_->check(trl_cuda_block_update(ctx_->handle(), dtype, w.data_, V0.data_, static_cast<int>(count), C, static_cast<std::int64_t>(N), blocksize), "project_out update");
-    }
+    if (!gram_.get()) gram_ = DeviceBuffer(ctx_, sizeof(double) * blocksize * blocksize);
+    ctx_->check(trl_cuda_project_out(ctx_->handle(), dtype, V0.data_, static_cast<int>(count), w.data_, static_cast<std::int64_t>(N), blocksize, mode, eta,
+                                     static_cast<double*>(gram_.get())),
+                "project_out");
+    gram_block_ = w.data_;
+    gram_seq_ = ctx_->seq();
   }
 
   Context& context() const { return *ctx_; }
@@ -126,7 +131,9 @@ protected:
   std::vector<Scalar> eigenvalues;
   std::unique_ptr<BlockMatrix> eigenvectors;
   DeviceBuffer evals_dev_;
-  DeviceBuffer coef_;
+  DeviceBuffer gram_;                  // Gram matrix of the last reorthogonalised block
+  const Storage* gram_block_ = nullptr; // ... which block it belongs to
+  std::uint64_t gram_seq_ = 0;         // ... and the operation sequence number it was made at
 
   Scalar tolerance_ = 1e-8;
   int cholqr_passes_ = 2;

@@ -80,8 +80,9 @@ uint64_t trl_cuda_launch_count(trl_cuda_handle handle);
  * When enabled, every outermost C-ABI call is bracketed by CUDA events on the handle's
  * stream and credited with its algorithmic bytes (data each operand must move once) and
  * flops. Classes: spmm, block_dot, block_update, block_rotate, bv_mult, cholqr, bv_sub,
- * small_eigen, copy, sddmm, block_ops. */
-#define TRL_PROF_CLASSES 11
+ * small_eigen, copy, sddmm, block_ops, reorth_pass2 (the conditional second Gram-Schmidt
+ * pass of trl_cuda_project_out: time only, no bytes). */
+#define TRL_PROF_CLASSES 12
 typedef struct trl_kernel_stats {
   char name[24];
   uint64_t calls;
@@ -159,6 +160,24 @@ int trl_cuda_block_dot_noalloc(void* stream, int dtype, const void* V, int nblk,
  * With trl_cuda_block_dot this is one classical Gram-Schmidt pass against nblk blocks,
  * replacing nblk rounds of ModifiedGS (reorthogonalization.hh:14-21). */
 int trl_cuda_block_update(trl_cuda_handle h, int dtype, void* W, const void* V, int nblk, const double* C, int64_t n, int bs);
+
+/* Classical Gram-Schmidt of W against V_0..V_{nblk-1}, fused for the reorthogonalisation
+ * step of the driver (replaces ModifiedGS, reorthogonalization.hh:14-21):
+ *   pass 1: C = V^T W (one multi-block dot), W -= V C (one update that also forms W^T W);
+ *   pass 2 (W -= V (V^T W) again): always for TRL_CGS_TWO; for TRL_CGS_IFNEEDED only when
+ *   a column kept less than `eta` of its norm through pass 1 (the DGKS criterion of
+ *   Daniel, Gragg, Kaufman & Stewart, 1976; eta = 1/sqrt(2) is customary), decided on the
+ *   device without a host round trip; never for TRL_CGS_ONE.
+ * G (device, bs x bs) receives W^T W of the result, for trl_cuda_cholqr_gram. When W is the
+ * block right after V_{nblk-1} (as in the driver) the Gram of the input rides along with
+ * pass 1's dot. */
+enum trl_cgs_mode { TRL_CGS_ONE = 0, TRL_CGS_TWO = 1, TRL_CGS_IFNEEDED = 2 };
+int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, int mode, double eta, double* G);
+
+/* trl_cuda_cholqr with the Gram matrix of the first pass supplied (G0 = X^T X on the device,
+ * e.g. from trl_cuda_project_out); each further pass forms its Gram matrix while it applies
+ * U^{-1}, so CholQR2 reads and writes X twice. G0 == NULL is trl_cuda_cholqr. */
+int trl_cuda_cholqr_gram(trl_cuda_handle h, int dtype, void* X, int64_t n, int bs, int passes, double* R, const double* G0);
 
 /* Thick-restart rotation W_j = sum_{i<m} V_i Y(i,j) for j < k, in one pass over V.
  * Y is a block matrix with ldy block columns (Y(i,j) at Y + (i*ldy + j)*bs*bs).

@@ -28,7 +28,9 @@ extern "C" {
 #endif
 
 enum trl_mode { TRL_MODE_FP64 = 0, TRL_MODE_FP32 = 1, TRL_MODE_MIXED = 2 };
-enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1 };
+/* Reorthogonalisation strategy: the reference's ModifiedGS, or the backend's block classical
+ * Gram-Schmidt variants (include/trl/impl/cuda/reorthogonalization.hh). */
+enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEEDED = 2, TRL_REORTH_CGS1 = 3 };
 
 typedef struct trl_solve_params {
   int bs;                        /* block size: 1, 2, 4, 8, 16 */

@@ -170,6 +170,71 @@ def test_cholqr2_orthonormal_and_factor(cuda_handle, bs, dtype):
     assert rel < (1e-12 if dtype == torch.float64 else 1e-6)
 
 
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("contiguous", [True, False])
+def test_project_out_modes(cuda_handle, bs, dtype, contiguous):
+    """trl_cuda_project_out against numpy classical Gram-Schmidt (one / two passes), its
+    returned Gram matrix, and the DGKS decision of the if-needed mode."""
+    rng = np.random.default_rng(7 * bs + contiguous)
+    n, nblk = 3001, 6
+    Q, _ = np.linalg.qr(rng.standard_normal((n, nblk * bs)))
+    V = as_dt(Q.reshape(n, nblk, bs).transpose(1, 0, 2).copy(), dtype)
+    eps = 1e-12 if dtype == torch.float64 else 2e-6
+
+    def run(w0, mode):
+        store = torch.zeros((nblk + 1, n, bs), dtype=dtype, device="cuda")
+        store[:nblk] = dev(V, dtype)
+        if contiguous:
+            Vd, Wd = store[:nblk], store[nblk]
+            Wd.copy_(dev(w0, dtype))
+        else:
+            Vd, Wd = dev(V, dtype), dev(w0, dtype)
+        G = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+        cuda_handle.project_out(Vd, Wd, mode, G)
+        return host(Wd), host(G)
+
+    Vf = V.transpose(1, 0, 2).reshape(n, nblk * bs)
+    # a vector with a large component in span(V): one pass loses orthogonality, two restore it
+    w = as_dt(Vf @ rng.standard_normal((nblk * bs, bs)) * 100 + rng.standard_normal((n, bs)), dtype)
+    w1 = w - Vf @ (Vf.T @ w)
+    w2 = w1 - Vf @ (Vf.T @ w1)
+    got1, G1 = run(w, native.TRL_CGS_ONE)
+    got2, G2 = run(w, native.TRL_CGS_TWO)
+    got3, G3 = run(w, native.TRL_CGS_IFNEEDED)
+    scale = np.abs(w).max()
+    close(got1, w1, scale, eps)
+    close(got2, w2, scale, eps)
+    close(got3, got2, scale, eps)  # large cancellation: the criterion asks for the second pass
+    close(G1, got1.T @ got1, np.abs(G1).max(), 1e-10)
+    close(G2, got2.T @ got2, np.abs(G2).max(), 1e-10)
+    assert np.abs(Vf.T @ got2).max() < 1e4 * eps * np.abs(got2).max()
+    # an almost orthogonal vector: the if-needed mode keeps one pass
+    w = as_dt(rng.standard_normal((n, bs)) + Vf @ rng.standard_normal((nblk * bs, bs)) * 1e-3, dtype)
+    got1, _ = run(w, native.TRL_CGS_ONE)
+    got3, G3 = run(w, native.TRL_CGS_IFNEEDED)
+    assert np.array_equal(got1, got3)
+    close(G3, got3.T @ got3, np.abs(G3).max(), 1e-10)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+def test_cholqr_with_given_gram_matches_cholqr(cuda_handle, bs, dtype):
+    rng = np.random.default_rng(bs + 5)
+    X = as_dt(rng.standard_normal((20_011, bs)), dtype)
+    X1, X2 = dev(X, dtype), dev(X, dtype)
+    R1 = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+    R2 = torch.zeros_like(R1)
+    G0 = torch.zeros_like(R1)
+    cuda_handle.block_dot(X2[None], X2, G0[None])
+    cuda_handle.cholqr(X1, 2, R1)
+    cuda_handle.cholqr_gram(X2, 2, R2, G0)
+    cuda_handle.sync()
+    tol = 1e-12 if dtype == torch.float64 else 1e-6
+    close(host(X2), host(X1), 1.0, tol)
+    close(host(R2), host(R1), np.abs(host(R1)).max(), tol)
+
+
 def test_cholqr_breakdown_is_reported(cuda_handle):
     Xd = torch.zeros((100, 4), dtype=torch.float64, device="cuda")
     Rd = torch.zeros((4, 4), dtype=torch.float64, device="cuda")

@@ -69,7 +69,7 @@ def cfg1_oracle(oracle):
     return A, X0, r
 
 
-@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS2, native.TRL_REORTH_MGS])
+@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS2, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS])
 @pytest.mark.parametrize("passes", [1, 2])
 def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
     A, X0, ref = cfg1_oracle

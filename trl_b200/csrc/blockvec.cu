@@ -82,8 +82,9 @@ __global__ void __launch_bounds__(kThreads) k_convert(D* __restrict__ dst, const
 // partial[row_chunk][j][BS*BS]; k_reduce_partials adds the row chunks in a fixed order.
 template <typename T, int BS, int JC, int G>
 __global__ void __launch_bounds__(kThreads) k_block_dot(const T* __restrict__ V, int64_t vstride, int nblk, const T* __restrict__ W, int64_t n, int64_t rows_per_cta,
-                                                        double* __restrict__ partial)
+                                                        double* __restrict__ partial, const int* __restrict__ cond = nullptr)
 {
+  if (cond && *cond == 0) return; // device-side skip (uniform over the grid)
   constexpr int NT = (BS + 7) / 8;
   constexpr int BB = BS * BS;
   __shared__ double red[kWarps][NT * NT * 64];
@@ -165,10 +166,149 @@ __global__ void __launch_bounds__(kThreads) k_block_dot(const T* __restrict__ V,
   }
 }
 
+// ---------------------------------------------------------------- block dot, bulk-copy pipeline
+// Same result as k_block_dot, for BS*sizeof(T) a multiple of 16 bytes. The CTA walks its
+// row range in tiles of R rows (4 KB per block tile). Thread 0 streams the W tile and the
+// tiles of the JC blocks of V into an S-stage shared-memory ring with 1-D bulk copies that
+// complete on a per-stage "full" mbarrier; the 8 warps read DMMA fragments from shared
+// memory and release the stage on its "empty" mbarrier. HBM traffic is a continuous stream
+// of 4 KB copies, independent of register pressure and of the element width.
+// Waits are bounded (mbar_wait): on a timeout the status word records TRL_DEV_TIMEOUT, the
+// threads leave the tile loop, and thread 0 waits (bounded) for the copies it issued.
+template <typename T, int BS, int TB>
+struct BulkTile {
+  static constexpr int R = TB / (BS * static_cast<int>(sizeof(T))); // rows per tile (TB bytes per block tile)
+  static constexpr int ELEMS = R * BS;
+};
+
+template <typename T, int BS, int JC, int S, int TB>
+__global__ void __launch_bounds__(kThreads) k_block_dot_bulk(const T* __restrict__ V, int64_t vstride, int nblk, const T* __restrict__ W, int64_t n, int64_t rows_per_cta,
+                                                             double* __restrict__ partial, int* status, const int* __restrict__ cond)
+{
+  if (cond && *cond == 0) return; // device-side skip (uniform over the grid)
+  constexpr int NT = (BS + 7) / 8;
+  constexpr int BB = BS * BS;
+  constexpr int R = BulkTile<T, BS, TB>::R;
+  constexpr int TILE = BulkTile<T, BS, TB>::ELEMS;
+  constexpr int GPW = R / (kWarps * 4); // 4-row groups per warp per tile
+  static_assert(GPW >= 1 && R % (kWarps * 4) == 0, "tile rows must cover the CTA's warps");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T* tiles = reinterpret_cast<T*>(smem_raw); // [S][JC + 1][TILE]: slot 0 is W
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(S) * (JC + 1) * TILE * sizeof(T));
+  uint64_t* empty = full + S;
+  __shared__ double red[kWarps][NT * NT * 64];
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int j0 = blockIdx.x * JC;
+  const int jn = min(JC, nblk - j0);
+  const int64_t rb = static_cast<int64_t>(blockIdx.y) * rows_per_cta;
+  const int64_t re = min(n, rb + rows_per_cta);
+  const int ntiles = re > rb ? static_cast<int>((re - rb + R - 1) / R) : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kWarps);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+
+  int issued = 0; // thread 0: tiles whose copies were started
+  auto issue = [&](int t) {
+    const int s = t % S;
+    const int64_t r0 = rb + static_cast<int64_t>(t) * R;
+    const uint32_t bytes = static_cast<uint32_t>(min(static_cast<int64_t>(R), re - r0) * BS * sizeof(T));
+    T* st = tiles + static_cast<size_t>(s) * (JC + 1) * TILE;
+    mbar_arrive_expect_tx(&full[s], bytes * static_cast<uint32_t>(jn + 1));
+    bulk_g2s(st, W + r0 * BS, bytes, &full[s]);
+    for (int jj = 0; jj < jn; ++jj) bulk_g2s(st + (jj + 1) * TILE, V + static_cast<int64_t>(j0 + jj) * vstride + r0 * BS, bytes, &full[s]);
+    issued = t + 1;
+  };
+  if (threadIdx.x == 0)
+    for (int t = 0; t < min(S - 1, ntiles); ++t) issue(t);
+
+  double acc[JC][NT][NT][2];
+#pragma unroll
+  for (int jj = 0; jj < JC; ++jj)
+#pragma unroll
+    for (int a = 0; a < NT; ++a)
+#pragma unroll
+      for (int b = 0; b < NT; ++b) acc[jj][a][b][0] = acc[jj][a][b][1] = 0.0;
+
+  int consumed = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    if (threadIdx.x == 0 && t + S - 1 < ntiles) {
+      const int tn = t + S - 1; // refill the slot that tile t-1 used
+      if (tn < S || mbar_wait(&empty[tn % S], static_cast<uint32_t>((tn - S) / S) & 1u, status)) issue(tn);
+    }
+    const int s = t % S;
+    if (!mbar_wait(&full[s], static_cast<uint32_t>(t / S) & 1u, status)) break;
+    const T* st = tiles + static_cast<size_t>(s) * (JC + 1) * TILE;
+    const int rows = static_cast<int>(min(static_cast<int64_t>(R), re - (rb + static_cast<int64_t>(t) * R)));
+#pragma unroll
+    for (int q = 0; q < GPW; ++q) {
+      const int lr = (warp * GPW + q) * 4 + t4;
+      const bool rok = lr < rows;
+      double bf[NT];
+#pragma unroll
+      for (int tk = 0; tk < NT; ++tk) {
+        const int col = tk * 8 + g;
+        bf[tk] = (rok && col < BS) ? static_cast<double>(st[lr * BS + col]) : 0.0;
+      }
+#pragma unroll
+      for (int jj = 0; jj < JC; ++jj) {
+        if (jj < jn) {
+#pragma unroll
+          for (int ti = 0; ti < NT; ++ti) {
+            const int col = ti * 8 + g;
+            const double a = (rok && col < BS) ? static_cast<double>(st[(jj + 1) * TILE + lr * BS + col]) : 0.0;
+#pragma unroll
+            for (int tk = 0; tk < NT; ++tk) dmma_m8n8k4(acc[jj][ti][tk][0], acc[jj][ti][tk][1], a, bf[tk]);
+          }
+        }
+      }
+    }
+    __syncwarp(); // the DMMAs above consumed every lane's shared-memory reads
+    if (lane == 0) mbar_arrive(&empty[s]);
+    consumed = t + 1;
+  }
+  if (threadIdx.x == 0) // after an aborted loop: let the copies already started land
+    for (int t = consumed; t < issued; ++t) mbar_wait(&full[t % S], static_cast<uint32_t>(t / S) & 1u, status, 1u << 20);
+
+#pragma unroll
+  for (int jj = 0; jj < JC; ++jj) {
+    if (jj >= jn) break;
+#pragma unroll
+    for (int ti = 0; ti < NT; ++ti)
+#pragma unroll
+      for (int tk = 0; tk < NT; ++tk) {
+        red[warp][(ti * NT + tk) * 64 + g * 8 + 2 * t4 + 0] = acc[jj][ti][tk][0];
+        red[warp][(ti * NT + tk) * 64 + g * 8 + 2 * t4 + 1] = acc[jj][ti][tk][1];
+      }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NT * NT * 64; e += kThreads) {
+      const int tile = e >> 6, within = e & 63;
+      const int row = (tile / NT) * 8 + (within >> 3);
+      const int col = (tile % NT) * 8 + (within & 7);
+      if (row < BS && col < BS) {
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) sum += red[w][e];
+        partial[(static_cast<int64_t>(blockIdx.y) * nblk + j0 + jj) * BB + row * BS + col] = sum;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // out[e] = sum_c partial[c][e]: 32 outputs per CTA, 8 slices of the chunk range per output
 // with four independent accumulators each (the loads overlap), combined in a fixed order.
-__global__ void __launch_bounds__(kThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out)
+__global__ void __launch_bounds__(kThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out,
+                                                              const int* __restrict__ cond = nullptr)
 {
+  if (cond && *cond == 0) return;
   __shared__ double part[8][33];
   const int o = threadIdx.x & 31, s = threadIdx.x >> 5;
   const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + o;
@@ -285,6 +425,241 @@ __global__ void __launch_bounds__(kThreads) k_block_gemm(const T* in, int64_t is
   }
 }
 
+// ---------------------------------------------------------------- update + Gram in one pass
+// out = (accumulate ? out : 0) + sign * sum_{i<MB} in_i Coef(i),  Coef(i) = coef + i*BS*BS,
+// and in the same pass the Gram matrix out^T out of the values as stored (rounded to T):
+// each warp stages its finished rows in shared memory, re-reads them in DMMA fragment
+// layout (k = rows) and accumulates the BS x BS Gram; per-CTA sums go to
+// gram_partial[blockIdx.x][BS*BS]. When cond is given and *cond == 0 the kernel does
+// nothing (a device-side decision: no host round trip). `in` and `out` may alias for MB = 1.
+template <typename T, int BS, int RT, int U>
+__global__ void __launch_bounds__(kThreads) k_update_gram(const T* in, int64_t istride, int MB, const double* __restrict__ coef, T* out, int64_t n, int accumulate, double sign,
+                                                          double* __restrict__ gram_partial, const int* __restrict__ cond)
+{
+  if (cond && *cond == 0) return;
+  constexpr int NT = (BS + 7) / 8;
+  constexpr int KS = (BS + 3) / 4;
+  __shared__ double stage[kWarps][RT * 8 * BS];
+  __shared__ double red[kWarps][NT * NT * 64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * kWarps + warp;
+  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * kWarps;
+  double gacc[NT][NT][2];
+#pragma unroll
+  for (int a = 0; a < NT; ++a)
+#pragma unroll
+    for (int b = 0; b < NT; ++b) gacc[a][b][0] = gacc[a][b][1] = 0.0;
+
+  for (int64_t r0 = warp_global * 8 * RT; r0 < n; r0 += warp_stride * 8 * RT) {
+    double acc[RT][NT][2];
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+      const int64_t row = r0 + r * 8 + g;
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int col = t * 8 + 2 * t4 + i;
+          acc[r][t][i] = (accumulate && row < n && col < BS) ? static_cast<double>(out[row * BS + col]) : 0.0;
+        }
+    }
+    for (int ib0 = 0; ib0 < MB; ib0 += U) {
+      double a[U][RT][KS];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const T* A = in + static_cast<int64_t>(min(ib0 + u, MB - 1)) * istride;
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+          const int64_t row = r0 + r * 8 + g;
+#pragma unroll
+          for (int ks = 0; ks < KS; ++ks) {
+            const int kcol = ks * 4 + t4;
+            a[u][r][ks] = (row < n && kcol < BS) ? static_cast<double>(A[row * BS + kcol]) : 0.0;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (ib0 + u < MB) {
+          const double* Cb = coef + static_cast<int64_t>(ib0 + u) * (BS * BS);
+#pragma unroll
+          for (int ks = 0; ks < KS; ++ks)
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+              const int krow = ks * 4 + t4, ncol = t * 8 + g;
+              const double b = (krow < BS && ncol < BS) ? sign * __ldg(Cb + krow * BS + ncol) : 0.0;
+#pragma unroll
+              for (int r = 0; r < RT; ++r) dmma_m8n8k4(acc[r][t][0], acc[r][t][1], a[u][r][ks], b);
+            }
+        }
+      }
+    }
+    // store, and stage the stored values for the Gram
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+      const int64_t row = r0 + r * 8 + g;
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int col = t * 8 + 2 * t4 + i;
+          if (col < BS) {
+            const T v = static_cast<T>(acc[r][t][i]);
+            if (row < n) out[row * BS + col] = v;
+            stage[warp][(r * 8 + g) * BS + col] = row < n ? static_cast<double>(v) : 0.0;
+          }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2 * RT; ++q) { // groups of 4 staged rows = the DMMA k dimension
+      const int lr = q * 4 + t4;
+      double bf[NT];
+#pragma unroll
+      for (int tk = 0; tk < NT; ++tk) bf[tk] = (tk * 8 + g < BS) ? stage[warp][lr * BS + tk * 8 + g] : 0.0;
+#pragma unroll
+      for (int ti = 0; ti < NT; ++ti) {
+        const double av = (ti * 8 + g < BS) ? stage[warp][lr * BS + ti * 8 + g] : 0.0;
+#pragma unroll
+        for (int tk = 0; tk < NT; ++tk) dmma_m8n8k4(gacc[ti][tk][0], gacc[ti][tk][1], av, bf[tk]);
+      }
+    }
+    __syncwarp();
+  }
+  // cross-warp reduction of the Gram
+#pragma unroll
+  for (int ti = 0; ti < NT; ++ti)
+#pragma unroll
+    for (int tk = 0; tk < NT; ++tk) {
+      red[warp][(ti * NT + tk) * 64 + g * 8 + 2 * t4 + 0] = gacc[ti][tk][0];
+      red[warp][(ti * NT + tk) * 64 + g * 8 + 2 * t4 + 1] = gacc[ti][tk][1];
+    }
+  __syncthreads();
+  for (int e = threadIdx.x; e < NT * NT * 64; e += kThreads) {
+    const int tile = e >> 6, within = e & 63;
+    const int row = (tile / NT) * 8 + (within >> 3);
+    const int col = (tile % NT) * 8 + (within & 7);
+    if (row < BS && col < BS) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) s += red[w][e];
+      gram_partial[static_cast<int64_t>(blockIdx.x) * BS * BS + row * BS + col] = s;
+    }
+  }
+}
+
+// DGKS criterion (Daniel, Gragg, Kaufman & Stewart 1976): a second Gram-Schmidt pass is
+// needed when some column kept less than eta of its norm through the first pass.
+template <int BS>
+__global__ void k_dgks_flag(const double* __restrict__ G_before, const double* __restrict__ G_after, double eta2, int* __restrict__ flag)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int f = 0;
+  for (int c = 0; c < BS; ++c) f |= (G_after[c * BS + c] < eta2 * G_before[c * BS + c]);
+  *flag = f;
+}
+
+// dst = *flag ? a : b  (BS x BS)
+__global__ void k_select_block(const int* __restrict__ flag, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ dst, int count)
+{
+  const int e = threadIdx.x;
+  if (e < count) dst[e] = *flag ? a[e] : b[e];
+}
+
+// ---------------------------------------------------------------- small Cholesky, one CTA
+// Gram matrix G from `chunks` partial sums (chunks = 0: G given), then G = L L^T reading
+// the lower triangle, Uinv = L^{-T} for the apply, and R <- L^T (first pass) or
+// R <- L^T R (so that X_in = X_out R across passes). All in shared memory; the factor and
+// the inverse are column-parallel over one warp. A pivot <= 0 (or NaN) records
+// TRL_DEV_CHOLESKY and writes Uinv = I, leaving the apply a no-op.
+template <int BS>
+__global__ void __launch_bounds__(kThreads) k_gram_factor(const double* __restrict__ src, int chunks, double* __restrict__ Uinv, double* __restrict__ R, int first, int* status)
+{
+  __shared__ double G[BS * BS], L[BS][BS + 1], Li[BS][BS + 1], Ro[BS * BS];
+  __shared__ double part[8][32];
+  __shared__ int bad;
+  const int tid = threadIdx.x;
+  // 1. G
+  if (chunks > 0) {
+    for (int e0 = 0; e0 < BS * BS; e0 += 32) {
+      const int o = tid & 31, s = tid >> 5, e = e0 + o;
+      double a = 0.0;
+      if (e < BS * BS)
+        for (int c = s; c < chunks; c += 8) a += src[static_cast<int64_t>(c) * BS * BS + e];
+      part[s][o] = a;
+      __syncthreads();
+      if (s == 0 && e < BS * BS) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t += part[q][o];
+        G[e] = t;
+      }
+      __syncthreads();
+    }
+  }
+  else {
+    for (int e = tid; e < BS * BS; e += kThreads) G[e] = src[e];
+  }
+  for (int e = tid; e < BS * BS; e += kThreads) Ro[e] = R[e];
+  if (tid == 0) bad = 0;
+  __syncthreads();
+  if (tid < 32) {
+    const int lane = tid;
+    // 2. L: column by column; lane i < BS owns row i
+    for (int j = 0; j < BS; ++j) {
+      if (lane == j) {
+        double d = G[j * BS + j];
+        for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
+        if (!(d > 0.0)) bad = 1;
+        L[j][j] = d > 0.0 ? sqrt(d) : 1.0;
+      }
+      __syncwarp();
+      if (lane > j && lane < BS) {
+        double s = G[lane * BS + j];
+        for (int k = 0; k < j; ++k) s -= L[lane][k] * L[j][k];
+        L[lane][j] = s / L[j][j];
+      }
+      if (lane < j) L[lane][j] = 0.0;
+      __syncwarp();
+    }
+    // 3. Li = L^{-1} (lower): lane c owns column c, forward substitution
+    if (lane < BS) {
+      const int c = lane;
+      for (int i = 0; i < BS; ++i) {
+        if (i < c) {
+          Li[i][c] = 0.0;
+          continue;
+        }
+        double s = (i == c) ? 1.0 : 0.0;
+        for (int k = c; k < i; ++k) s -= L[i][k] * Li[k][c];
+        Li[i][c] = s / L[i][i];
+      }
+    }
+    __syncwarp();
+    // 4. outputs: Uinv = Li^T; R (lane i owns row i)
+    if (lane < BS) {
+      const int i = lane;
+      for (int c = 0; c < BS; ++c) Uinv[i * BS + c] = bad ? (i == c ? 1.0 : 0.0) : Li[c][i];
+      if (!bad) {
+        for (int c = 0; c < BS; ++c) {
+          double s;
+          if (first) {
+            s = (c >= i) ? L[c][i] : 0.0;
+          }
+          else {
+            s = 0.0;
+            for (int k = i; k <= c; ++k) s += L[k][i] * Ro[k * BS + c];
+            if (c < i) s = 0.0;
+          }
+          R[i * BS + c] = s;
+        }
+      }
+    }
+    if (lane == 0 && bad) atomicOr(status, TRL_DEV_CHOLESKY);
+  }
+}
+
 // ---------------------------------------------------------------- small Cholesky
 // G = U^T U (lower triangle of G read, as an LL^T factorisation); writes U^{-1} for the
 // apply and folds U into R (R <- U on the first pass, R <- U R afterwards, so that
@@ -357,7 +732,7 @@ using namespace trl_detail;
 namespace trl_detail {
 
 template <typename T, int BS, int JC, int G>
-int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C)
+int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C, const int* cond)
 {
   const int64_t len = static_cast<int64_t>(nblk) * BS * BS;
   const int gj = (nblk + JC - 1) / JC;
@@ -374,26 +749,102 @@ int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, i
   double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
   if (!partial) return TRL_ENOMEM;
   dim3 grid(gj, static_cast<unsigned>(chunks));
-  k_block_dot<T, BS, JC, G><<<grid, kThreads, 0, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial);
+  k_block_dot<T, BS, JC, G><<<grid, kThreads, 0, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C);
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
-// Chooses the block chunk JC (accumulators per warp) and the row groups G per iteration so
-// that every warp keeps about 16-20 independent loads in flight.
-template <typename T, int BS>
-int launch_block_dot(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C)
+template <typename T, int BS, int JC, int S, int TB>
+int launch_block_dot_bulk(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C, const int* cond)
 {
-  if (n == 0) {
+  constexpr int R = BulkTile<T, BS, TB>::R;
+  constexpr size_t smem = static_cast<size_t>(S) * (JC + 1) * BulkTile<T, BS, TB>::ELEMS * sizeof(T) + 2 * S * sizeof(uint64_t);
+  static int resident = 0; // CTAs per SM at this shared-memory size (queried once)
+  if (resident == 0) {
+    cudaFuncSetAttribute(k_block_dot_bulk<T, BS, JC, S, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_block_dot_bulk<T, BS, JC, S, TB>, kThreads, smem) != cudaSuccess || resident < 1) resident = 1;
+    cudaGetLastError();
+  }
+  const int64_t len = static_cast<int64_t>(nblk) * BS * BS;
+  const int gj = (nblk + JC - 1) / JC;
+  int64_t chunks = static_cast<int64_t>(h->num_sms) * resident / gj;
+  if (chunks < 1) chunks = 1;
+  const int64_t max_chunks = (n + 2 * R - 1) / (2 * R); // at least two tiles per CTA
+  if (chunks > max_chunks) chunks = max_chunks;
+  int64_t rows_per_cta = (n + chunks - 1) / chunks;
+  rows_per_cta = (rows_per_cta + R - 1) / R * R;
+  chunks = (n + rows_per_cta - 1) / rows_per_cta;
+  double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
+  if (!partial) return TRL_ENOMEM;
+  k_block_dot_bulk<T, BS, JC, S, TB><<<dim3(gj, static_cast<unsigned>(chunks)), kThreads, smem, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial, h->d_status, cond);
+  int st = after_launch(h, "block_dot");
+  if (st) return st;
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
+  return after_launch(h, "block_dot reduce");
+}
+
+// Bulk-copy pipeline when a row of the block is a whole number of 16-byte units; otherwise
+// the register-prefetch kernel with JC blocks and G row groups per warp iteration (about
+// 16-20 independent loads in flight per warp).
+template <typename T, int BS>
+int launch_block_dot(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C, const int* cond = nullptr)
+{
+  if (n == 0 && !cond) {
     cudaMemsetAsync(C, 0, static_cast<size_t>(nblk) * BS * BS * sizeof(double), h->stream);
     return TRL_OK;
   }
-  if (nblk == 1) return launch_block_dot_jc<T, BS, 1, 8>(h, V, nblk, W, n, C);
-  if (nblk == 2) return launch_block_dot_jc<T, BS, 2, 4>(h, V, nblk, W, n, C);
-  if (nblk <= 4) return launch_block_dot_jc<T, BS, 4, (BS >= 16 ? 2 : 4)>(h, V, nblk, W, n, C);
-  return launch_block_dot_jc<T, BS, (BS >= 16 ? 4 : 8), 2>(h, V, nblk, W, n, C);
+  // Shapes measured on B200 for the 884,736 x 8 blocks of the 96^3 workload (GB/s of
+  // algorithmic bytes; the STREAM copy reference is 6,552): FP64 with 2 KB tiles, JC=8, S=3
+  // gives 6,662 (24 blocks) and 6,970 (48 blocks); FP32 with 4 KB tiles gives 4,371 (8),
+  // 5,269 (24) and with JC=4 5,804 (48).
+  if constexpr ((BS * sizeof(T)) % 16 == 0) {
+    constexpr int TBS = (BS * sizeof(T) <= 64) ? 2048 : 4096; // small tiles where 32 rows fit
+    constexpr int JCL = BS >= 16 ? 4 : 8;
+    if (nblk == 1) return launch_block_dot_bulk<T, BS, 1, 8, 4096>(h, V, nblk, W, n, C, cond);
+    if (nblk == 2) return launch_block_dot_bulk<T, BS, 2, 6, 4096>(h, V, nblk, W, n, C, cond);
+    if (nblk <= 4) return launch_block_dot_bulk<T, BS, 4, 4, 4096>(h, V, nblk, W, n, C, cond);
+    if constexpr (sizeof(T) == 8) return launch_block_dot_bulk<T, BS, JCL, 3, TBS>(h, V, nblk, W, n, C, cond);
+    if (nblk <= 8) return launch_block_dot_bulk<T, BS, JCL, 3, 4096>(h, V, nblk, W, n, C, cond);
+    return launch_block_dot_bulk<T, BS, 4, 3, TBS>(h, V, nblk, W, n, C, cond);
+  }
+  if (nblk == 1) return launch_block_dot_jc<T, BS, 1, 8>(h, V, nblk, W, n, C, cond);
+  if (nblk == 2) return launch_block_dot_jc<T, BS, 2, 4>(h, V, nblk, W, n, C, cond);
+  if (nblk <= 4) return launch_block_dot_jc<T, BS, 4, (BS >= 16 ? 2 : 4)>(h, V, nblk, W, n, C, cond);
+  return launch_block_dot_jc<T, BS, (BS >= 16 ? 4 : 8), 2>(h, V, nblk, W, n, C, cond);
+}
+
+// Launches k_update_gram; the per-CTA Gram partial sums are left in the workspace
+// (*partial, *chunks) for the caller to reduce.
+template <typename T, int BS>
+int launch_update_gram_partials(trl_cuda_context* h, const T* in, int MB, const double* coef, T* out, int64_t n, int accumulate, double sign, const int* cond,
+                                double** partial, int* chunks)
+{
+  constexpr int NT = (BS + 7) / 8;
+  constexpr int KS = (BS + 3) / 4;
+  constexpr int RT = NT >= 2 ? 1 : 2;
+  constexpr int U = KS >= 4 ? 2 : 4;
+  const unsigned grid = grid_for(h, (n + 8 * RT - 1) / (8 * RT), kWarps, 4);
+  *partial = static_cast<double*>(workspace(h, static_cast<size_t>(grid) * BS * BS * sizeof(double)));
+  *chunks = static_cast<int>(grid);
+  if (!*partial) return TRL_ENOMEM;
+  if (MB == 1) // a single input block: no point loading it U times
+    k_update_gram<T, BS, RT, 1><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
+  else
+    k_update_gram<T, BS, RT, U><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
+  return after_launch(h, "update_gram");
+}
+
+template <typename T, int BS>
+int launch_update_gram(trl_cuda_context* h, const T* in, int MB, const double* coef, T* out, int64_t n, int accumulate, double sign, double* G, const int* cond)
+{
+  double* partial = nullptr;
+  int chunks = 0;
+  int st = launch_update_gram_partials<T, BS>(h, in, MB, coef, out, n, accumulate, sign, cond, &partial, &chunks);
+  if (st) return st;
+  k_reduce_partials<<<(BS * BS + 31) / 32, kThreads, 0, h->stream>>>(partial, chunks, BS * BS, G, cond);
+  return after_launch(h, "update_gram reduce");
 }
 
 template <typename T, int BS, int NBMAX>
@@ -404,7 +855,10 @@ void launch_gemm_nb(trl_cuda_context* h, const T* in, int MB, const double* coef
   constexpr int RT = (NBMAX * NT >= 8) ? 1 : 2; // keep the accumulators within ~64 registers
   constexpr int U = (KS >= 4) ? 2 : 4;
   const unsigned grid = grid_for(h, (n + 8 * RT - 1) / (8 * RT), kWarps, 8);
-  k_block_gemm<T, BS, NBMAX, RT, U><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
+  if (MB == 1) // a single input block: no point loading it U times
+    k_block_gemm<T, BS, NBMAX, RT, 1><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
+  else
+    k_block_gemm<T, BS, NBMAX, RT, U><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
 }
 
 template <typename T, int BS>
@@ -575,18 +1029,107 @@ int trl_cuda_cholqr(trl_cuda_handle h, int dtype, void* X, int64_t n, int bs, in
   double* small = static_cast<double*>(small_scratch(h));
   if (!small) return TRL_ENOMEM;
   double* G = small;
-  double* Uinv = small + 256;
   ProfScope prof(h, PROF_CHOLQR, 3.0 * passes * n * bs * elt_size(dtype), 4.0 * passes * n * bs * bs);
+  int st = trl_cuda_block_dot(h, dtype, X, 1, X, n, bs, G);
+  if (st) return st;
+  return trl_cuda_cholqr_gram(h, dtype, X, n, bs, passes, R, G);
+}
+
+// Per pass: one-CTA factor of the Gram matrix, then the apply X <- X U^{-1}, which also
+// forms the partial Gram sums of the result for the next pass's factor.
+int trl_cuda_cholqr_gram(trl_cuda_handle h, int dtype, void* X, int64_t n, int bs, int passes, double* R, const double* G0)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!G0) return trl_cuda_cholqr(h, dtype, X, n, bs, passes, R);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (passes < 1 || passes > 4) return set_error(h, TRL_EINVAL, "passes must be in [1, 4]");
+  if (!X || !R) return set_error(h, TRL_EINVAL, "null pointer");
+  double* small = static_cast<double*>(small_scratch(h));
+  if (!small) return TRL_ENOMEM;
+  double* Uinv = small + 256;
+  ProfScope prof(h, PROF_CHOLQR, 2.0 * passes * n * bs * elt_size(dtype), 4.0 * passes * n * bs * bs);
+  const double* src = G0; // the Gram matrix, or per-CTA partial sums of it
+  int chunks = 0;
   for (int p = 0; p < passes; ++p) {
-    int st = trl_cuda_block_dot(h, dtype, X, 1, X, n, bs, G);
-    if (st) return st;
-    TRL_DISPATCH_BS(bs, k_chol_factor<BS><<<1, 32, 0, h->stream>>>(G, Uinv, R, p == 0, h->d_status));
+    int st = TRL_OK;
+    TRL_DISPATCH_BS(bs, k_gram_factor<BS><<<1, kThreads, 0, h->stream>>>(src, chunks, Uinv, R, p == 0, h->d_status));
     st = after_launch(h, "cholqr factor");
     if (st) return st;
-    TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(X), 1, Uinv, 1, 0, static_cast<T*>(X), 1, n, 0, 1.0)));
+    if (p + 1 < passes) {
+      double* partial = nullptr;
+      TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_update_gram_partials<T, BS>(h, static_cast<const T*>(X), 1, Uinv, static_cast<T*>(X), n, 0, 1.0, nullptr, &partial, &chunks)));
+      src = partial;
+    }
+    else {
+      TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(X), 1, Uinv, 1, 0, static_cast<T*>(X), 1, n, 0, 1.0)));
+    }
     if (st) return st;
   }
   return TRL_OK;
+}
+
+int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, int mode, double eta, double* G)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (nblk <= 0 || !G) return set_error(h, TRL_EINVAL, "bad project_out arguments");
+  if (mode != TRL_CGS_ONE && mode != TRL_CGS_TWO && mode != TRL_CGS_IFNEEDED) return set_error(h, TRL_EINVAL, "bad project_out mode %d", mode);
+  const int BB = bs * bs;
+  if (n == 0) return trl_cuda_memset_zero(h, G, sizeof(double) * BB);
+  if (!V || !W) return set_error(h, TRL_EINVAL, "null pointer");
+  const size_t es = elt_size(dtype);
+  // coefficient storage: C1 (nblk+1 blocks) | C2 (nblk blocks) | Gw0 | Gw1 | Gw2 | flag
+  double* base = static_cast<double*>(workspace2(h, sizeof(double) * (static_cast<size_t>(2 * nblk + 4) * BB) + 64));
+  if (!base) return TRL_ENOMEM;
+  double* C1 = base;
+  double* C2 = C1 + static_cast<size_t>(nblk + 1) * BB;
+  double* Gw0 = C2 + static_cast<size_t>(nblk) * BB;
+  double* Gw1 = Gw0 + BB;
+  double* Gw2 = Gw1 + BB;
+  int* flag = reinterpret_cast<int*>(Gw2 + BB);
+  const bool contiguous = static_cast<const char*>(W) == static_cast<const char*>(V) + static_cast<size_t>(nblk) * n * bs * es;
+  int st = TRL_OK;
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
+    const T* Vt = static_cast<const T*>(V);
+    T* Wt = static_cast<T*>(W);
+    // pass 1: C1 = V^T w (and w^T w, for free when w is the block right after V)
+    {
+      ProfScope prof(h, PROF_DOT, (nblk + (contiguous ? 1.0 : 2.0)) * n * bs * es, 2.0 * (nblk + 1) * n * bs * bs);
+      if (contiguous) {
+        st = launch_block_dot<T, BS>(h, Vt, nblk + 1, Wt, n, C1);
+        if (!st) st = trl_cuda_memcpy(h, Gw0, C1 + static_cast<size_t>(nblk) * BB, sizeof(double) * BB, TRL_D2D);
+      }
+      else {
+        st = launch_block_dot<T, BS>(h, Vt, nblk, Wt, n, C1);
+        if (!st) st = launch_block_dot<T, BS>(h, Wt, 1, Wt, n, Gw0);
+      }
+    }
+    if (st) return st;
+    {
+      ProfScope prof(h, PROF_UPDATE, (nblk + 2.0) * n * bs * es, 2.0 * nblk * n * bs * bs + 2.0 * n * bs * bs);
+      st = launch_update_gram<T, BS>(h, Vt, nblk, C1, Wt, n, 1, -1.0, Gw1, nullptr);
+    }
+    if (st) return st;
+    if (mode == TRL_CGS_ONE) return trl_cuda_memcpy(h, G, Gw1, sizeof(double) * BB, TRL_D2D);
+    if (mode == TRL_CGS_TWO) {
+      cudaMemsetAsync(flag, 0x01, sizeof(int), h->stream);
+    }
+    else {
+      k_dgks_flag<BS><<<1, 32, 0, h->stream>>>(Gw0, Gw1, eta * eta, flag);
+      if ((st = after_launch(h, "dgks"))) return st;
+    }
+    // pass 2, only where the flag is set (decided on the device; its bytes are not credited
+    // to the profile because the host does not know whether it ran)
+    {
+      ProfScope prof(h, PROF_REORTH2, 0.0);
+      st = launch_block_dot<T, BS>(h, Vt, nblk, Wt, n, C2, flag);
+      if (!st) st = launch_update_gram<T, BS>(h, Vt, nblk, C2, Wt, n, 1, -1.0, Gw2, flag);
+    }
+    if (st) return st;
+    k_select_block<<<1, 256, 0, h->stream>>>(flag, Gw2, Gw1, G, BB);
+    st = after_launch(h, "select");
+  }));
+  return st;
 }
 
 } // extern "C"

@@ -21,7 +21,9 @@ struct trl_cuda_context {
   cudaStream_t stream = nullptr;
   bool owns_stream = false;
   int* d_status = nullptr;  // device status word
-  void* ws = nullptr;       // growable device workspace
+  void* ws = nullptr;       // growable device workspace (per-call partial sums)
+  void* ws2 = nullptr;      // growable device workspace (coefficients kept across calls of one operation)
+  size_t ws2_bytes = 0;
   double* d_small = nullptr; // 1024 doubles of fixed scratch (Gram / factor blocks)
   size_t ws_bytes = 0;
   int* pinned_status = nullptr; // pinned host copy of d_status
@@ -51,6 +53,7 @@ int set_error(trl_cuda_context* h, int status, const char* fmt, ...);
 
 // Ensures at least `bytes` of device workspace; returns nullptr and sets an error on failure.
 void* workspace(trl_cuda_context* h, size_t bytes);
+void* workspace2(trl_cuda_context* h, size_t bytes);
 void* pinned(trl_cuda_context* h, size_t bytes);
 
 inline bool valid_bs(int bs) { return bs == 1 || bs == 2 || bs == 4 || bs == 8 || bs == 16; }
@@ -65,7 +68,7 @@ void* small_scratch(trl_cuda_context* h);
 void destroy_solver(trl_cuda_context* h);
 
 // Kernel classes of the profiler (index into trl_cuda_context::prof).
-enum ProfClass { PROF_SPMM = 0, PROF_DOT, PROF_UPDATE, PROF_ROTATE, PROF_MULT, PROF_CHOLQR, PROF_SUB, PROF_SMALL_EIGEN, PROF_COPY, PROF_SDDMM, PROF_BLOCK_OPS };
+enum ProfClass { PROF_SPMM = 0, PROF_DOT, PROF_UPDATE, PROF_ROTATE, PROF_MULT, PROF_CHOLQR, PROF_SUB, PROF_SMALL_EIGEN, PROF_COPY, PROF_SDDMM, PROF_BLOCK_OPS, PROF_REORTH2 };
 
 cudaEvent_t prof_event(trl_cuda_context* h);
 // Folds completed timings into the per-class totals (after a stream synchronisation).
@@ -130,6 +133,49 @@ template <typename T>
 __device__ __forceinline__ double ld_widen(const T* p)
 {
   return static_cast<double>(__ldg(p));
+}
+
+// ---- bulk-copy pipeline primitives (sm_90+ PTX; no cluster multicast anywhere) ------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// makes mbarrier initialisation visible to the asynchronous (bulk-copy) proxy
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
+{
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Waits for the phase with the given parity to complete. Bounded: after `limit` polls it
+// records TRL_DEV_TIMEOUT in the status word and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status, uint32_t limit = (1u << 24))
+{
+  const uint32_t a = smem_addr(bar);
+  for (uint32_t it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(a), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  atomicOr(status, TRL_DEV_TIMEOUT);
+  return false;
+}
+
+// 1-D bulk copy global -> shared, completing `bytes` transactions on `bar`. Both addresses
+// 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
 }
 
 #define TRL_CHECK_HANDLE(h)                                                                                                                                                                            \

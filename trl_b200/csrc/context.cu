@@ -47,6 +47,25 @@ void* workspace(trl_cuda_context* h, size_t bytes)
   return h->ws;
 }
 
+void* workspace2(trl_cuda_context* h, size_t bytes)
+{
+  if (bytes <= h->ws2_bytes) return h->ws2;
+  if (h->ws2) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->ws2);
+    h->ws2 = nullptr;
+    h->ws2_bytes = 0;
+  }
+  size_t want = bytes < 65536 ? 65536 : bytes + bytes / 4;
+  if (cudaMalloc(&h->ws2, want) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(h, TRL_ENOMEM, "workspace allocation of %zu bytes failed", want);
+    return nullptr;
+  }
+  h->ws2_bytes = want;
+  return h->ws2;
+}
+
 void* pinned(trl_cuda_context* h, size_t bytes)
 {
   if (bytes <= h->pinned_bytes) return h->pinned;
@@ -103,7 +122,7 @@ void prof_resolve(trl_cuda_context* h)
 using namespace trl_detail;
 
 static const char* kProfNames[TRL_PROF_CLASSES] = {"spmm", "block_dot", "block_update", "block_rotate", "bv_mult", "cholqr",
-                                                    "bv_sub", "small_eigen", "copy", "sddmm", "block_ops"};
+                                                    "bv_sub", "small_eigen", "copy", "sddmm", "block_ops", "reorth_pass2"};
 
 extern "C" int trl_cuda_profile_enable(trl_cuda_handle h, int on)
 {
@@ -188,6 +207,7 @@ int trl_cuda_destroy(trl_cuda_handle h)
   for (cudaEvent_t e : h->prof_free) cudaEventDestroy(e);
   destroy_solver(h);
   if (h->ws) cudaFree(h->ws);
+  if (h->ws2) cudaFree(h->ws2);
   if (h->d_small) cudaFree(h->d_small);
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->d_status) cudaFree(h->d_status);

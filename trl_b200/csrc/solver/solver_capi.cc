@@ -119,8 +119,12 @@ template <class Storage, unsigned bs>
 PhaseOut run_phase_r(const std::shared_ptr<Context>& ctx, const trl_csr* A, const trl_solve_params& p, unsigned max_restarts, double tol, const Storage* X0, unsigned kx,
                      Storage* ritz_out)
 {
-  if (p.reorth == TRL_REORTH_MGS) return run_phase<Storage, bs, trl::ModifiedGS>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
-  return run_phase<Storage, bs, trl::cuda::BlockCGS2>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
+  switch (p.reorth) {
+  case TRL_REORTH_MGS: return run_phase<Storage, bs, trl::ModifiedGS>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
+  case TRL_REORTH_CGS2: return run_phase<Storage, bs, trl::cuda::BlockCGS2>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
+  case TRL_REORTH_CGS1: return run_phase<Storage, bs, trl::cuda::BlockCGS1>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
+  default: return run_phase<Storage, bs, trl::cuda::BlockCGSIfNeeded>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
+  }
 }
 
 template <unsigned bs>
@@ -248,6 +252,7 @@ void validate(const trl_solve_params* p)
   if (p->mode < TRL_MODE_FP64 || p->mode > TRL_MODE_MIXED) throw std::invalid_argument("bad mode");
   if (p->ncv % p->bs != 0) throw std::invalid_argument("ncv must be a multiple of the block size");
   if (p->cholqr_passes < 1 || p->cholqr_passes > 4) throw std::invalid_argument("cholqr_passes must be in [1, 4]");
+  if (p->reorth < TRL_REORTH_MGS || p->reorth > TRL_REORTH_CGS1) throw std::invalid_argument("bad reorth strategy");
 }
 
 } // namespace
@@ -266,7 +271,7 @@ void trl_solve_params_default(trl_solve_params* p)
   p->tol = 1e-8;
   p->alpha = 1.0;
   p->beta = 0.0;
-  p->reorth = TRL_REORTH_CGS2;
+  p->reorth = TRL_REORTH_CGS_IFNEEDED;
   p->cholqr_passes = 2;
   p->fp32_tol = 1e-5;
   p->refine_max_restarts = 1000;

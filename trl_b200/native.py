@@ -23,7 +23,8 @@ TRL_F64, TRL_F32 = 0, 1
 TRL_H2D, TRL_D2H, TRL_D2D = 0, 1, 2
 TRL_MULT, TRL_MULT_TRANSPOSE, TRL_MULT_ADD, TRL_SUBTRACT = 0, 1, 2, 3
 TRL_MODE_FP64, TRL_MODE_FP32, TRL_MODE_MIXED = 0, 1, 2
-TRL_REORTH_MGS, TRL_REORTH_CGS2 = 0, 1
+TRL_REORTH_MGS, TRL_REORTH_CGS2, TRL_REORTH_CGS_IFNEEDED, TRL_REORTH_CGS1 = 0, 1, 2, 3
+TRL_CGS_ONE, TRL_CGS_TWO, TRL_CGS_IFNEEDED = 0, 1, 2
 
 P = C.c_void_p
 I64 = C.c_int64
@@ -52,6 +53,8 @@ CUDA_SYMBOLS = {
     "trl_cuda_block_update": (C.c_int, [P, C.c_int, P, P, C.c_int, P, I64, C.c_int]),
     "trl_cuda_block_rotate": (C.c_int, [P, C.c_int, P, C.c_int, P, C.c_int, C.c_int, P, I64, C.c_int]),
     "trl_cuda_cholqr": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P]),
+    "trl_cuda_cholqr_gram": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P, P]),
+    "trl_cuda_project_out": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, C.c_int, C.c_double, P]),
     "trl_cuda_spmm": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double]),
     "trl_cuda_csr_norm1": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "trl_cuda_sddmm": (C.c_int, [P, P, P, C.c_int, P, P]),
@@ -64,7 +67,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_profile_read": (C.c_int, [P, P]),
 }
 
-TRL_PROF_CLASSES = 11
+TRL_PROF_CLASSES = 12
 
 
 class trl_kernel_stats(C.Structure):
@@ -223,6 +226,14 @@ class Handle:
     def cholqr(self, X, passes: int, R):
         n, bs = X.shape
         self.check(self.lib.trl_cuda_cholqr(self.h, _dtype(X), _ptr(X), n, bs, passes, _ptr(R)))
+
+    def project_out(self, V, W, mode: int, G, eta: float = 0.7071067811865476):
+        nblk, n, bs = V.shape
+        self.check(self.lib.trl_cuda_project_out(self.h, _dtype(V), _ptr(V), nblk, _ptr(W), n, bs, mode, eta, _ptr(G)))
+
+    def cholqr_gram(self, X, passes: int, R, G0):
+        n, bs = X.shape
+        self.check(self.lib.trl_cuda_cholqr_gram(self.h, _dtype(X), _ptr(X), n, bs, passes, _ptr(R), _ptr(G0)))
 
     def convert(self, dst, src):
         self.check(self.lib.trl_cuda_convert(self.h, _dtype(dst), _ptr(dst), _dtype(src), _ptr(src), src.numel()))
