@@ -207,6 +207,20 @@ int trl_cuda_csr_norm1(trl_cuda_handle h, const trl_csr* A, double alpha, double
  * No counterpart in the reference (it has no derivatives). */
 int trl_cuda_sddmm(trl_cuda_handle h, const trl_csr* pattern, const double* X, int k, const double* w, double* out);
 
+/* Adjoint of a weighted eigenvalue sum f = sum_c w[c] lambda[c] with respect to the stored
+ * entries of the operator (no counterpart in the reference, which has no derivatives).
+ * X: n x k row-major FP64 (device), the eigenvectors, normalised in the problem's inner
+ * product (x^T x = 1, or x^T M x = 1 for K x = lambda M x); host_evals / host_weights: k
+ * values on the host. Eigenvalues closer than cluster_rtol * max|lambda| are one cluster;
+ * inside a cluster the weights are replaced by their mean, which makes f's gradient
+ * independent of the basis chosen inside the degenerate eigenspace (the projector of a
+ * cluster is well defined; its individual eigenvectors are not).
+ *   kind = 0: grad[p] = df/dA_ij  = sum_c wbar[c] x_c[i] x_c[j]            (A, or K)
+ *   kind = 1: grad[p] = df/dM_ij  = -sum_c wbar[c] lambda[c] x_c[i] x_c[j] (mass M)
+ * for every stored entry p = (i, j) of `pattern` (values unused). */
+int trl_cuda_eigen_adjoint(trl_cuda_handle h, const trl_csr* pattern, const double* X, int k, const double* host_evals, const double* host_weights, double cluster_rtol,
+                           int kind, double* grad);
+
 /* ---- small bs x bs block operations (impl/openmp/matrixblockview.hh:30-74) ---------- */
 int trl_cuda_mb_copy(trl_cuda_handle h, double* dst, const double* src, int bs, int transpose); /* :30-46 */
 int trl_cuda_mb_zero(trl_cuda_handle h, double* dst, int bs);                                   /* :48-52 */

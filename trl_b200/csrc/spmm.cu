@@ -9,7 +9,10 @@
 // mode, as the FP32 SpMM is specified; FP64 otherwise).
 #include "common.cuh"
 
+#include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <vector>
 
 namespace {
 
@@ -233,6 +236,47 @@ int trl_cuda_sddmm(trl_cuda_handle h, const trl_csr* P, const double* X, int k, 
   const unsigned grid = grid_for(h, P->n, kThreads / 32, 16);
   k_sddmm<<<grid, kThreads, 0, h->stream>>>(P->n, P->rowptr, P->colind, X, k, w, out);
   return after_launch(h, "sddmm");
+}
+
+int trl_cuda_eigen_adjoint(trl_cuda_handle h, const trl_csr* P, const double* X, int k, const double* host_evals, const double* host_weights, double cluster_rtol, int kind,
+                           double* grad)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!P || !X || !host_evals || !host_weights || !grad) return set_error(h, TRL_EINVAL, "null pointer");
+  if (k <= 0 || k > 4096) return set_error(h, TRL_EINVAL, "k must be in [1, 4096]");
+  if (kind != 0 && kind != 1) return set_error(h, TRL_EINVAL, "kind must be 0 (operator) or 1 (mass)");
+  if (cluster_rtol < 0.0) return set_error(h, TRL_EINVAL, "negative cluster tolerance");
+  // cluster-averaged coefficients (host; k is small). Eigenvalues are grouped by sorting and
+  // joining neighbours closer than cluster_rtol * max|lambda|.
+  std::vector<double> c(k);
+  std::vector<int> order(k);
+  double amax = 0.0;
+  for (int i = 0; i < k; ++i) {
+    order[i] = i;
+    amax = std::fmax(amax, std::fabs(host_evals[i]));
+  }
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return host_evals[a] < host_evals[b]; });
+  const double gap = cluster_rtol * amax;
+  for (int s = 0; s < k;) {
+    int e = s + 1;
+    while (e < k && host_evals[order[e]] - host_evals[order[e - 1]] <= gap) ++e;
+    double mean = 0.0;
+    for (int q = s; q < e; ++q) mean += host_weights[order[q]];
+    mean /= (e - s);
+    for (int q = s; q < e; ++q) {
+      const int i = order[q];
+      c[i] = kind == 0 ? mean : -mean * host_evals[i];
+    }
+    s = e;
+  }
+  double* dc = static_cast<double*>(workspace2(h, sizeof(double) * k));
+  if (!dc) return TRL_ENOMEM;
+  if (int st = trl_cuda_memcpy(h, dc, c.data(), sizeof(double) * k, TRL_H2D)) return st;
+  if (int st = trl_cuda_sddmm(h, P, X, k, dc, grad)) return st;
+  // the host coefficient array goes out of scope: make sure the copy has been consumed
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return set_error(h, TRL_ECUDA, "eigen_adjoint: %s", cudaGetErrorString(e));
+  return TRL_OK;
 }
 
 } // extern "C"

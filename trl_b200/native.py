@@ -58,6 +58,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_spmm": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double]),
     "trl_cuda_csr_norm1": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "trl_cuda_sddmm": (C.c_int, [P, P, P, C.c_int, P, P]),
+    "trl_cuda_eigen_adjoint": (C.c_int, [P, P, P, C.c_int, P, P, C.c_double, C.c_int, P]),
     "trl_cuda_mb_copy": (C.c_int, [P, P, P, C.c_int, C.c_int]),
     "trl_cuda_mb_zero": (C.c_int, [P, P, C.c_int]),
     "trl_cuda_mb_mult": (C.c_int, [P, P, P, P, C.c_int]),
@@ -250,6 +251,16 @@ class Handle:
     def sddmm(self, A: "DeviceCSRTensors", X, w, out):
         n, k = X.shape
         self.check(self.lib.trl_cuda_sddmm(self.h, C.byref(A.desc), _ptr(X), k, _ptr(w), _ptr(out)))
+
+    def eigen_adjoint(self, pattern: "DeviceCSRTensors", X, evals: np.ndarray, weights: np.ndarray, grad, kind: int = 0,
+                      cluster_rtol: float = 1e-8):
+        """grad[p] = d(sum_c w_c lambda_c)/d(entry p) over the CSR pattern (kind 0: operator /
+        stiffness entries; kind 1: mass entries), cluster-averaged weights."""
+        n, k = X.shape
+        ev = np.ascontiguousarray(evals, dtype=np.float64)
+        wt = np.ascontiguousarray(weights, dtype=np.float64)
+        self.check(self.lib.trl_cuda_eigen_adjoint(self.h, C.byref(pattern.desc), _ptr(X), k, ev.ctypes.data, wt.ctypes.data,
+                                                   cluster_rtol, kind, _ptr(grad)))
 
     def small_eigen(self, T, beta, nev: int, tol: float):
         """T: block matrix (nblk, nblk, bs, bs) float64 on the device."""
