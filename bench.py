@@ -236,16 +236,12 @@ def trl_arm(args, world, rank, local):
 
     # ---- roofline of the dominant kernel class (live, over the profiled FP64 solve) ----
     hbm, bf16, src = peaks()
-    kern = {}
-    for name, s in prof.items():
-        if s["calls"] == 0:
-            continue
-        kern[name] = {"calls": s["calls"], "seconds": s["seconds"], "share": None, "bytes_per_call": s["bytes"] / s["calls"],
-                      "gbs": s["bytes"] / s["seconds"] / 1e9 if s["seconds"] > 0 else None,
-                      "tflops": s["flops"] / s["seconds"] / 1e12 if s["seconds"] > 0 else None}
-    tot = sum(v["seconds"] for v in kern.values())
-    for v in kern.values():
-        v["share"] = v["seconds"] / tot if tot else None
+    kern = breakdown(prof)
+    # the same breakdown for an FP32-mode solve to the mixed mode's FP32 tolerance
+    h.profile(True)
+    solve32 = native.solve_csr_device(h, A64, A32, X0d, evecs=evecs, mode=native.TRL_MODE_FP32, **dict(common, tol=args.fp32_tol))
+    kern32 = breakdown(h.profile_read())
+    h.profile(False)
     dominant = max(kern, key=lambda k: kern[k]["seconds"])
     d = kern[dominant]
     # achieved = algorithmic bytes per call / mean call duration (CUDA events on the solver's
@@ -280,6 +276,7 @@ def trl_arm(args, world, rank, local):
             "spmm": {"gbs": spmm.get("gbs"), "frac_of_hbm": (spmm.get("gbs") or 0) / hbm, "calls": spmm.get("calls"),
                      "bytes_per_call": 6137856 * 12 + 4 * 884737 + 2 * 884736 * 8 * 8},
             "kernels": kern,
+            "kernels_fp32": {"restarts": solve32["restarts"], "seconds": solve32["seconds"], "classes": kern32},
             "roofline": roofline,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(e2e["h2d_bytes"]), "d2h_bytes_per_step": int(e2e["d2h_bytes"]),
                     "api": "trl_solve_csr_host (pinned host CSR + start block in, eigenvalues + eigenvectors out)"},
@@ -293,6 +290,21 @@ def trl_arm(args, world, rank, local):
         dist.barrier()
         dist.destroy_process_group()
     return result
+
+
+def breakdown(prof: dict) -> dict:
+    """Per kernel class: calls, device seconds, share, algorithmic bytes per call, GB/s, TF/s."""
+    kern = {}
+    for name, s in prof.items():
+        if s["calls"] == 0:
+            continue
+        kern[name] = {"calls": s["calls"], "seconds": s["seconds"], "share": None, "bytes_per_call": s["bytes"] / s["calls"],
+                      "gbs": s["bytes"] / s["seconds"] / 1e9 if s["seconds"] > 0 else None,
+                      "tflops": s["flops"] / s["seconds"] / 1e12 if s["seconds"] > 0 else None}
+    tot = sum(v["seconds"] for v in kern.values())
+    for v in kern.values():
+        v["share"] = v["seconds"] / tot if tot else None
+    return kern
 
 
 def load_traffic(kernel: str, algorithmic_bytes_per_call: float):

@@ -28,28 +28,28 @@ public:
   /// A = B                                   (matrixblockview.hh:30-33)
   void copy_from(BlockMatrixBlockView other)
   {
-    ctx_->flush();
+    ctx_->prepare({{other.data_, kBytes, false}, {data_, kBytes, true}});
     ctx_->check(trl_cuda_mb_copy(ctx_->handle(), data_, other.data_, block_size, 0), "copy_from");
   }
 
   /// A = B^T                                 (matrixblockview.hh:39-43)
   void copy_from_transpose(BlockMatrixBlockView other)
   {
-    ctx_->flush();
+    ctx_->prepare({{other.data_, kBytes, false}, {data_, kBytes, true}});
     ctx_->check(trl_cuda_mb_copy(ctx_->handle(), data_, other.data_, block_size, 1), "copy_from_transpose");
   }
 
   /// A = 0                                   (matrixblockview.hh:49)
   void set_zero()
   {
-    ctx_->flush();
+    ctx_->prepare({{data_, kBytes, true}});
     ctx_->check(trl_cuda_mb_zero(ctx_->handle(), data_, block_size), "set_zero");
   }
 
   /// C = A B                                 (matrixblockview.hh:55-64)
   void mult(BlockMatrixBlockView B, BlockMatrixBlockView C) const
   {
-    ctx_->flush();
+    ctx_->prepare({{data_, kBytes, false}, {B.data_, kBytes, false}, {C.data_, kBytes, true}});
     ctx_->check(trl_cuda_mb_mult(ctx_->handle(), data_, B.data_, C.data_, block_size), "mult");
   }
 
@@ -57,12 +57,15 @@ public:
   void set_diagonal(std::span<double> values)
   {
     if (values.size() < block_size) throw std::invalid_argument("set_diagonal: need blocksize values");
-    ctx_->flush();
+    ctx_->prepare({{data_, kBytes, false}, {data_, kBytes, true}});
     ctx_->check(trl_cuda_mb_set_diagonal(ctx_->handle(), data_, values.data(), block_size), "set_diagonal");
   }
 
   Context* ctx_;
   double* data_; // device pointer
+
+private:
+  static constexpr std::size_t kBytes = sizeof(double) * block_size * block_size;
 };
 
 template <unsigned int block_size>

@@ -34,46 +34,33 @@ public:
   /// X = Y                                   blockview.hh:59-63
   void copy_from(BlockView other)
   {
-    ctx_->flush();
+    ctx_->prepare({{other.data_, bytes(), false}, {data_, bytes(), true}});
     ctx_->check(trl_cuda_bv_copy(ctx_->handle(), dtype, data_, other.data_, static_cast<std::int64_t>(n_), block_size), "copy_from");
   }
 
   /// X -= Y                                  blockview.hh:69-74
   BlockView& operator-=(BlockView other)
   {
-    ctx_->flush();
-    ctx_->check(trl_cuda_bv_sub(ctx_->handle(), dtype, data_, other.data_, static_cast<std::int64_t>(n_), block_size), "operator-=");
+    ctx_->record_sub(dtype, block_size, static_cast<std::int64_t>(n_), data_, other.data_);
     return *this;
   }
 
   /// other += X W (recorded; see Context)   blockview.hh:81-97
   void mult_add(MatrixBlockView W, BlockView other) { ctx_->record_mult_add(dtype, block_size, static_cast<std::int64_t>(n_), data_, W.data_, other.data_); }
 
-  /// other = X W                             blockview.hh:104-119
-  void mult(MatrixBlockView W, BlockView other)
-  {
-    ctx_->flush();
-    ctx_->check(trl_cuda_bv_mult(ctx_->handle(), dtype, TRL_MULT, data_, W.data_, other.data_, static_cast<std::int64_t>(n_), block_size), "mult");
-  }
+  /// other = X W (recorded; see Context)    blockview.hh:104-119
+  void mult(MatrixBlockView W, BlockView other) { ctx_->record_mult(dtype, block_size, static_cast<std::int64_t>(n_), data_, W.data_, other.data_, false); }
 
-  /// other = X W^T                           blockview.hh:126-141
-  void mult_transpose(MatrixBlockView W, BlockView other)
-  {
-    ctx_->flush();
-    ctx_->check(trl_cuda_bv_mult(ctx_->handle(), dtype, TRL_MULT_TRANSPOSE, data_, W.data_, other.data_, static_cast<std::int64_t>(n_), block_size), "mult_transpose");
-  }
+  /// other = X W^T (recorded; see Context)  blockview.hh:126-141
+  void mult_transpose(MatrixBlockView W, BlockView other) { ctx_->record_mult(dtype, block_size, static_cast<std::int64_t>(n_), data_, W.data_, other.data_, true); }
 
-  /// R = X^T other (FP64, deterministic)     blockview.hh:152-182
-  void dot(BlockView other, MatrixBlockView R)
-  {
-    ctx_->flush();
-    ctx_->check(trl_cuda_block_dot(ctx_->handle(), dtype, data_, 1, other.data_, static_cast<std::int64_t>(n_), block_size, R.data_), "dot");
-  }
+  /// R = X^T other (FP64, deterministic; recorded, see Context)   blockview.hh:152-182
+  void dot(BlockView other, MatrixBlockView R) { ctx_->record_dot(dtype, block_size, static_cast<std::int64_t>(n_), data_, other.data_, R.data_); }
 
   /// X -= other R                            blockview.hh:189-201
   void subtract_product(BlockView other, MatrixBlockView R)
   {
-    ctx_->flush();
+    ctx_->prepare({{other.data_, bytes(), false}, {R.data_, sizeof(double) * block_size * block_size, false}, {data_, bytes(), false}, {data_, bytes(), true}});
     ctx_->check(trl_cuda_bv_mult(ctx_->handle(), dtype, TRL_SUBTRACT, other.data_, R.data_, data_, static_cast<std::int64_t>(n_), block_size), "subtract_product");
   }
 
@@ -82,6 +69,8 @@ public:
 
 private:
   std::size_t n_;
+
+  std::size_t bytes() const { return sizeof(Storage) * n_ * block_size; }
 };
 
 } // namespace trl::cuda

@@ -4,7 +4,8 @@
 // Context: owns the C-ABI handle (include/trl_cuda.h: one CUDA stream + device workspace),
 // turns non-zero ABI status codes into the exception types the reference throws
 // (std::invalid_argument, std::runtime_error with the reference's messages,
-// impl/openmp/evp_base.hh:55,96), and batches the restart rotation.
+// impl/openmp/evp_base.hh:55,96), and defers two call patterns of the driver so that they
+// can be fused.
 //
 // Rotation batching. The thick restart (lanczos.hh:105-114) issues, for every kept block j,
 // W_j.set_zero() followed by m calls V_i.mult_add(Y_ij, W_j): k*m passes that each re-read
@@ -14,10 +15,28 @@
 // block matrix Y", it is issued as one trl_cuda_block_rotate (one pass over V); otherwise
 // the calls are replayed one by one in their original order. Results are identical up to
 // floating-point summation order.
+//
+// Three-term fusion. Every block Lanczos step (lanczos.hh:243-262; after a restart
+// :167-183) reduces W = A V_i against its neighbours before the full reorthogonalisation:
+// W0 = V_{i-1} beta^T, W -= W0, T_ii = V_i^T W, W0 = V_i T_ii, W -= W0 (W0 a temporary
+// block). The context records these mult / mult_transpose / -= / dot calls and issues them
+// when the next operation of another kind arrives, in order, with every "product into a
+// temporary, then subtract the temporary" pair issued as one W -= X M kernel (three block
+// passes instead of five). The arithmetic is that of the calls one by one; only the
+// temporary's write is deferred. (Folding the step into the Gram-Schmidt projection that
+// follows would save more, but a single projection pass over the unreduced W loses
+// orthogonality geometrically: the step is the first of two effective passes.)
+//
+// Deferred writes. The temporary's last product (W0 = V_i T_ii) is written only if a later
+// operation reads W0, writes part of it, or writes V_i or T_ii first; it is dropped when an
+// operation overwrites all of W0 (the driver's next step does). Operations state what they
+// read and write through prepare(); flush() writes everything. Code that calls the C ABI
+// directly on this context's handle must call flush() first.
 #include "trl_cuda.h"
 
 #include <cstddef>
 #include <cstdint>
+#include <initializer_list>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -102,7 +121,14 @@ public:
     void* out;
   };
 
-  /// Enables or disables rotation batching (enabled by default).
+  /// Memory an operation reads or writes (device addresses; for deferred writes).
+  struct Access {
+    const void* ptr;
+    std::size_t bytes;
+    bool write;
+  };
+
+  /// Enables or disables rotation batching and three-term fusion (enabled by default).
   void set_batching(bool on)
   {
     flush();
@@ -112,7 +138,12 @@ public:
 
   void record_zero(int dtype, int bs, std::int64_t n, void* out)
   {
+    const std::size_t blk = block_bytes(dtype, bs, n);
+    replay_terms();
+    guard({{out, blk, true}});
     if (!batching_) {
+      ++seq_;
+      flush_rotation();
       check(trl_cuda_bv_zero(h_, dtype, out, n, bs), "set_zero");
       return;
     }
@@ -121,11 +152,90 @@ public:
 
   void record_mult_add(int dtype, int bs, std::int64_t n, const void* in, const double* coef, void* out)
   {
+    const std::size_t blk = block_bytes(dtype, bs, n);
+    replay_terms();
+    guard({{in, blk, false}, {coef, coef_bytes(bs), false}, {out, blk, false}, {out, blk, true}});
     if (!batching_) {
+      ++seq_;
+      flush_rotation();
       check(trl_cuda_bv_mult(h_, dtype, TRL_MULT_ADD, in, coef, out, n, bs), "mult_add");
       return;
     }
     push({1, dtype, bs, n, in, coef, out});
+  }
+
+  // ---- three-term calls (recorded for fusion) -----------------------------------------
+  // A record holds calls on one block w and one temporary t in the driver's grammar
+  // (mult into t, then w -= t; dots of basis blocks with w). A call that does not continue
+  // the record first issues it; a call that cannot start one runs at once.
+
+  /// t = x m (transpose: t = x m^T)                      BlockView::mult / mult_transpose
+  void record_mult(int dtype, int bs, std::int64_t n, const void* x, const double* m, void* t, bool transpose)
+  {
+    ++seq_;
+    const std::size_t blk = block_bytes(dtype, bs, n);
+    flush_rotation();
+    const TermOp op{transpose ? kMultT : kMult, dtype, bs, n, x, m, t, nullptr, nullptr};
+    const bool starts = batching_ && !overlaps(x, blk, t, blk);
+    const bool continues = starts && !terms_.empty() && same_shape(terms_.front(), op) && !is_mult(terms_.back()) && (!term_t_ || term_t_ == t) &&
+                           (!term_w_ || (!overlaps(t, blk, term_w_, blk) && !overlaps(x, blk, term_w_, blk)));
+    if (!continues) replay_terms();
+    guard({{x, blk, false}, {m, coef_bytes(bs), false}, {t, blk, true}});
+    if (!starts) {
+      run(op);
+      return;
+    }
+    terms_.push_back(op);
+    term_t_ = t;
+  }
+
+  /// w -= t                                              BlockView::operator-=
+  void record_sub(int dtype, int bs, std::int64_t n, void* w, const void* t)
+  {
+    ++seq_;
+    const std::size_t blk = block_bytes(dtype, bs, n);
+    flush_rotation();
+    const TermOp op{kSub, dtype, bs, n, nullptr, nullptr, const_cast<void*>(t), w, nullptr};
+    const bool continues = batching_ && !terms_.empty() && is_mult(terms_.back()) && terms_.back().t == t && same_shape(terms_.front(), op) &&
+                           (!term_w_ || term_w_ == w) && !overlaps(w, blk, t, blk) && !overlaps(w, blk, terms_.back().x, blk);
+    if (!continues) replay_terms();
+    guard({{w, blk, false}, {w, blk, true}, {t, blk, false}});
+    if (!continues) {
+      run(op);
+      return;
+    }
+    terms_.push_back(op);
+    term_w_ = w;
+  }
+
+  /// r = x^T w                                           BlockView::dot
+  void record_dot(int dtype, int bs, std::int64_t n, const void* x, const void* w, double* r)
+  {
+    ++seq_;
+    const std::size_t blk = block_bytes(dtype, bs, n);
+    flush_rotation();
+    const TermOp op{kDot, dtype, bs, n, x, nullptr, nullptr, const_cast<void*>(w), r};
+    const bool starts = batching_ && !overlaps(x, blk, w, blk);
+    const bool continues = starts && !terms_.empty() && same_shape(terms_.front(), op) && !is_mult(terms_.back()) && (!term_w_ || term_w_ == w) &&
+                           (!term_t_ || (!overlaps(w, blk, term_t_, blk) && !overlaps(x, blk, term_t_, blk)));
+    if (!continues) replay_terms();
+    guard({{x, blk, false}, {w, blk, false}, {r, coef_bytes(bs), true}});
+    if (!starts) {
+      run(op);
+      return;
+    }
+    terms_.push_back(op);
+    term_w_ = const_cast<void*>(w);
+  }
+
+  /// Before an operation that states the memory it reads and writes: writes or drops the
+  /// deferred product as needed and issues every recorded call.
+  void prepare(std::initializer_list<Access> acc)
+  {
+    ++seq_;
+    replay_terms();
+    flush_rotation();
+    guard(acc);
   }
 
   /// Operation sequence number: advances with every backend operation (each one flushes or
@@ -133,10 +243,137 @@ public:
   /// nothing ran in between.
   std::uint64_t seq() const { return seq_; }
 
-  /// Executes every recorded operation (fused when the pattern allows).
+  /// Executes every recorded and deferred operation (fused when the pattern allows).
   void flush()
   {
     ++seq_;
+    replay_terms();
+    flush_rotation();
+    if (has_deferred_) write_deferred();
+  }
+
+  /// Number of fused rotations issued so far (diagnostics).
+  std::uint64_t fused_rotations() const { return fused_; }
+  /// Number of product/subtract pairs issued as one kernel (diagnostics).
+  std::uint64_t fused_pairs() const { return fused_pairs_; }
+  /// Number of deferred products that had to be written (diagnostics).
+  std::uint64_t deferred_writes() const { return deferred_written_; }
+
+private:
+  enum { kMult = 0, kMultT = 1, kSub = 2, kDot = 3 };
+  struct TermOp {
+    int kind;
+    int dtype;
+    int bs;
+    std::int64_t n;
+    const void* x;   // mult / dot: basis block
+    const double* m; // mult: coefficient block
+    void* t;         // mult: product (temporary); sub: subtrahend
+    void* w;         // sub: w -= t; dot: r = x^T w
+    double* r;       // dot: result block
+  };
+
+  trl_cuda_handle h_ = nullptr;
+  bool owns_ = true;
+  bool batching_ = true;
+  std::vector<Op> pending_;
+  std::vector<TermOp> terms_;
+  void* term_w_ = nullptr; // the block the recorded three-term calls reduce
+  void* term_t_ = nullptr; // their temporary
+  TermOp deferred_{};
+  bool has_deferred_ = false;
+  std::uint64_t fused_ = 0;
+  std::uint64_t fused_pairs_ = 0;
+  std::uint64_t deferred_written_ = 0;
+  std::uint64_t seq_ = 0;
+
+  static std::size_t block_bytes(int dtype, int bs, std::int64_t n)
+  {
+    return static_cast<std::size_t>(n) * static_cast<std::size_t>(bs) * (dtype == TRL_F64 ? sizeof(double) : sizeof(float));
+  }
+  static std::size_t coef_bytes(int bs) { return sizeof(double) * static_cast<std::size_t>(bs) * static_cast<std::size_t>(bs); }
+  static bool overlaps(const void* a, std::size_t na, const void* b, std::size_t nb)
+  {
+    const auto pa = reinterpret_cast<std::uintptr_t>(a), pb = reinterpret_cast<std::uintptr_t>(b);
+    return na > 0 && nb > 0 && pa < pb + nb && pb < pa + na;
+  }
+  static bool is_mult(const TermOp& op) { return op.kind == kMult || op.kind == kMultT; }
+  static bool same_shape(const TermOp& a, const TermOp& b) { return a.dtype == b.dtype && a.bs == b.bs && a.n == b.n; }
+
+  void run(const TermOp& op)
+  {
+    switch (op.kind) {
+    case kMult: check(trl_cuda_bv_mult(h_, op.dtype, TRL_MULT, op.x, op.m, op.t, op.n, op.bs), "mult"); break;
+    case kMultT: check(trl_cuda_bv_mult(h_, op.dtype, TRL_MULT_TRANSPOSE, op.x, op.m, op.t, op.n, op.bs), "mult_transpose"); break;
+    case kSub: check(trl_cuda_bv_sub(h_, op.dtype, op.w, op.t, op.n, op.bs), "operator-="); break;
+    default: check(trl_cuda_block_dot(h_, op.dtype, op.x, 1, op.w, op.n, op.bs, op.r), "dot"); break;
+    }
+  }
+
+  /// Issues the recorded three-term calls in order; "t = x m, w -= t" pairs become one
+  /// w -= x m kernel and t = x m a deferred write. Each call is first checked against the
+  /// deferred product (which may have been made by an earlier pair of the same record).
+  void replay_terms()
+  {
+    if (terms_.empty()) return;
+    std::vector<TermOp> ops;
+    ops.swap(terms_);
+    term_w_ = term_t_ = nullptr;
+    for (std::size_t p = 0; p < ops.size(); ++p) {
+      const TermOp& op = ops[p];
+      const std::size_t blk = block_bytes(op.dtype, op.bs, op.n), cb = coef_bytes(op.bs);
+      if (is_mult(op) && p + 1 < ops.size() && ops[p + 1].kind == kSub && ops[p + 1].t == op.t && !overlaps(ops[p + 1].w, blk, op.x, blk) &&
+          !overlaps(ops[p + 1].w, blk, op.t, blk)) {
+        void* w = ops[p + 1].w;
+        if (has_deferred_ && deferred_.t == op.t) has_deferred_ = false; // overwritten by this product
+        guard({{op.x, blk, false}, {op.m, cb, false}, {w, blk, false}, {w, blk, true}});
+        if (has_deferred_) write_deferred(); // keep one deferred product at a time
+        check(trl_cuda_bv_mult(h_, op.dtype, op.kind == kMultT ? TRL_SUBTRACT_TRANSPOSE : TRL_SUBTRACT, op.x, op.m, w, op.n, op.bs), "operator-=");
+        deferred_ = op;
+        has_deferred_ = true;
+        ++fused_pairs_;
+        ++p;
+        continue;
+      }
+      switch (op.kind) {
+      case kMult:
+      case kMultT: guard({{op.x, blk, false}, {op.m, cb, false}, {op.t, blk, true}}); break;
+      case kSub: guard({{op.w, blk, false}, {op.w, blk, true}, {op.t, blk, false}}); break;
+      default: guard({{op.x, blk, false}, {op.w, blk, false}, {op.r, cb, true}}); break;
+      }
+      run(op);
+    }
+  }
+
+  void write_deferred()
+  {
+    has_deferred_ = false;
+    ++deferred_written_;
+    run(deferred_);
+  }
+
+  /// The deferred product commutes with everything recorded after it; an operation that
+  /// reads its output, writes part of it, or writes its inputs needs it written first; one
+  /// that overwrites all of its output (and reads none of it) makes it dead.
+  void guard(std::initializer_list<Access> acc)
+  {
+    if (!has_deferred_) return;
+    const TermOp& d = deferred_;
+    const std::size_t blk = block_bytes(d.dtype, d.bs, d.n), cb = coef_bytes(d.bs);
+    bool conflict = false, overwritten = false;
+    for (const auto& a : acc) {
+      if (a.write && (overlaps(a.ptr, a.bytes, d.x, blk) || overlaps(a.ptr, a.bytes, d.m, cb))) conflict = true;
+      if (overlaps(a.ptr, a.bytes, d.t, blk)) {
+        if (a.write && a.ptr == d.t && a.bytes >= blk) overwritten = true;
+        else conflict = true;
+      }
+    }
+    if (conflict) write_deferred();
+    else if (overwritten) has_deferred_ = false;
+  }
+
+  void flush_rotation()
+  {
     if (pending_.empty()) return;
     std::vector<Op> ops;
     ops.swap(pending_);
@@ -147,23 +384,12 @@ public:
     }
   }
 
-  /// Number of fused rotations issued so far (diagnostics).
-  std::uint64_t fused_rotations() const { return fused_; }
-
-private:
-  trl_cuda_handle h_ = nullptr;
-  bool owns_ = true;
-  bool batching_ = true;
-  std::vector<Op> pending_;
-  std::uint64_t fused_ = 0;
-  std::uint64_t seq_ = 0;
-
   void push(const Op& op)
   {
     ++seq_;
     if (!pending_.empty()) {
       const Op& f = pending_.front();
-      if (f.dtype != op.dtype || f.bs != op.bs || f.n != op.n) flush();
+      if (f.dtype != op.dtype || f.bs != op.bs || f.n != op.n) flush_rotation();
     }
     pending_.push_back(op);
   }

@@ -83,7 +83,8 @@ public:
 
   void apply(BlockView X, BlockView Y) override
   {
-    this->ctx_->flush();
+    const std::size_t blk = sizeof(Storage) * this->N * bs;
+    this->ctx_->prepare({{X.data_, blk, false}, {Y.data_, blk, true}});
     this->ctx_->check(trl_cuda_spmm(this->ctx_->handle(), A_.desc(), Base::dtype, X.data_, Y.data_, bs, alpha_, beta_), "apply");
     ++applies_;
   }

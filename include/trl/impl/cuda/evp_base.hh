@@ -58,7 +58,8 @@ public:
     // very block formed it (and no other operation ran since).
     const bool reuse = gram_block_ == V.data_ && gram_seq_ == ctx_->seq();
     gram_block_ = nullptr;
-    ctx_->flush();
+    const std::size_t blk = sizeof(Storage) * N * blocksize;
+    ctx_->prepare({{V.data_, blk, false}, {V.data_, blk, true}, {R.data_, kCoefBytes, true}});
     const double* G0 = reuse ? static_cast<const double*>(gram_.get()) : nullptr;
     ctx_->check(trl_cuda_cholqr_gram(ctx_->handle(), dtype, V.data_, static_cast<std::int64_t>(N), blocksize, cholqr_passes_, R.data_, G0), "orthonormalize");
   }
@@ -71,13 +72,16 @@ public:
 
   virtual std::size_t solve_small_dense(const BlockMatrix& B, BlockMatrixBlockView beta, std::size_t nev)
   {
-    ctx_->flush();
     const std::size_t nblk = B.block_rows();
     const std::size_t n_total = nblk * blocksize;
     if (!eigenvectors || eigenvectors->block_rows() != nblk) {
       eigenvectors = std::make_unique<BlockMatrix>(ctx_, nblk, nblk);
       evals_dev_ = DeviceBuffer(ctx_, sizeof(double) * n_total);
     }
+    ctx_->prepare({{B.data(), kCoefBytes * B.block_rows() * B.block_cols(), false},
+                   {beta.data_, kCoefBytes, false},
+                   {eigenvectors->data(), kCoefBytes * nblk * nblk, true},
+                   {evals_dev_.get(), sizeof(double) * n_total, true}});
     eigenvalues.resize(n_total);
     int nconv = 0;
     ctx_->check(trl_cuda_small_eigen(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
@@ -111,8 +115,9 @@ public:
   void project_out(BlockView V0, unsigned int count, BlockView w, int mode, double eta = 0.70710678118654752)
   {
     if (count == 0) return;
-    ctx_->flush();
     if (!gram_.get()) gram_ = DeviceBuffer(ctx_, sizeof(double) * blocksize * blocksize);
+    const std::size_t blk = sizeof(Storage) * N * blocksize;
+    ctx_->prepare({{V0.data_, blk * count, false}, {w.data_, blk, false}, {w.data_, blk, true}});
     ctx_->check(trl_cuda_project_out(ctx_->handle(), dtype, V0.data_, static_cast<int>(count), w.data_, static_cast<std::int64_t>(N), blocksize, mode, eta,
                                      static_cast<double*>(gram_.get())),
                 "project_out");
@@ -125,6 +130,8 @@ public:
   const double* device_eigenvalues() const { return static_cast<const double*>(evals_dev_.get()); }
 
 protected:
+  static constexpr std::size_t kCoefBytes = sizeof(double) * blocksize * blocksize;
+
   std::shared_ptr<Context> ctx_;
   std::size_t N;
 

@@ -115,7 +115,8 @@ enum trl_mult_mode {
   TRL_MULT = 0,           /* Y  = X W      blockview.hh:104-119 */
   TRL_MULT_TRANSPOSE = 1, /* Y  = X W^T    blockview.hh:126-141 */
   TRL_MULT_ADD = 2,       /* Y += X W      blockview.hh:81-97   */
-  TRL_SUBTRACT = 3        /* Y -= X W      blockview.hh:189-201 */
+  TRL_SUBTRACT = 3,       /* Y -= X W      blockview.hh:189-201 */
+  TRL_SUBTRACT_TRANSPOSE = 4 /* Y -= X W^T  (a mult_transpose and a -= in one pass, lanczos.hh:243-245) */
 };
 /* Y (op)= X * W with W a device bs x bs FP64 block. The reference's
  * Xv.subtract_product(Yv, R) (Xv -= Yv R) is trl_cuda_bv_mult(h, dt, TRL_SUBTRACT, Yv, R, Xv, n, bs). */

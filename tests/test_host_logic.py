@@ -3,6 +3,8 @@
 * trl::cuda::Context's batching of the thick-restart rotation (include/trl/impl/cuda/context.hh)
   against a fake C ABI: the pattern of lanczos.hh:105-114 becomes one trl_cuda_block_rotate;
   any other sequence is replayed call by call in its original order.
+* Its three-term fusion (lanczos.hh:243-262): product/subtract pairs become one kernel, the
+  temporary's write is deferred, and written exactly when a later operation needs it.
 * The C-ABI libraries load without a GPU and export every function include/*.h declares.
 * The multi-rank reduction bench.py uses (max over ranks) on a 2-rank gloo group.
 """
@@ -46,6 +48,32 @@ def test_single_input_block_and_flush_on_shape_change(batching_output):
     assert line(batching_output, "case6") == "case6 2 rotate zero"
     assert line(batching_output, "case7") == "case7 1"
     assert line(batching_output, "fused") == "fused 3"
+
+
+def test_three_term_step_runs_fused_with_its_temporary_deferred(batching_output):
+    # nothing is issued while the driver's step is recorded; the projection issues it as
+    # W -= V_{i-1} beta^T (one kernel), the dot, W -= V_i T_ii (one kernel)
+    assert line(batching_output, "case8a") == "case8a 0"
+    got = line(batching_output, "case8").split(" ", 1)[1]
+    assert got == line(batching_output, "expect8").split(" ", 1)[1]
+    # the deferred W0 survives unrelated operations and is dropped by the next step's overwrite
+    assert line(batching_output, "case8b") == "case8b 3 0 4"
+
+
+def test_deferred_product_is_written_before_it_is_needed(batching_output):
+    got = line(batching_output, "case9").split(" ", 2)
+    assert got[1] == "1" and got[2] == line(batching_output, "expect9").split(" ", 1)[1]
+    assert line(batching_output, "case10") == "case10 1 mult 0"
+    assert line(batching_output, "case10b") == "case10b 0"
+    # the restart step: dot, two fused subtractions, and flush() writes the last product
+    assert re.fullmatch(r"case11 4 dot \d+,mult 3,mult 4,mult 1,", line(batching_output, "case11"))
+
+
+def test_reference_modified_gs_and_unbatched_calls(batching_output):
+    # ModifiedGS's dot joins the record; its subtract_product issues everything in order
+    assert re.fullmatch(r"case12 4 mult 4,dot \d+,mult 3,dot \d+,", line(batching_output, "case12"))
+    # batching off: every call runs at once, nothing is fused
+    assert line(batching_output, "case7b") == "case7b 5"
 
 
 def _declared(header):

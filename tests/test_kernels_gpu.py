@@ -107,6 +107,10 @@ def test_block_view_ops_match_reference(cuda_handle, oracle, bs, dtype, n):
     Zd = dev(X, dtype)
     cuda_handle.bv_mult(native.TRL_SUBTRACT, dev(Y, dtype), Wd, Zd)
     close(host(Zd), Z, scale, tol)
+    # Y -= X W^T: mult_transpose followed by -= (lanczos.hh:243-245) in one pass
+    Zd = dev(X, dtype)
+    cuda_handle.bv_mult(native.TRL_SUBTRACT_TRANSPOSE, dev(Y, dtype), Wd, Zd)
+    close(host(Zd), X - Y @ W.T, scale, tol)
     # operator-=  (blockview.hh:69-74)
     Z = X.copy()
     oracle.block_view_op(bs, oracle.OP_SUB, Z, Y.copy(), W.copy())

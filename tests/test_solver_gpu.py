@@ -86,6 +86,23 @@ def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
     assert abs(out["restarts"] - ref["iterations"]) <= max(3, ref["iterations"] // 5)
 
 
+@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS])
+def test_fused_and_call_by_call_execution_agree(cfg1_oracle, reorth):
+    """batching = 1 fuses the three-term step's product/subtract pairs (deferring the
+    temporary) and the restart rotation; batching = 0 issues every driver call as its own
+    kernel. Both must give the reference's eigenpairs."""
+    A, X0, ref = cfg1_oracle
+    outs = [native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8, reorth=reorth, batching=b) for b in (0, 1)]
+    for out in outs:
+        assert out["converged"]
+        assert np.max(np.abs(out["evals"] - ref["evals"][:10]) / np.abs(ref["evals"][:10])) < 1e-10
+        assert np.max(out["resid"]) < 5e-8
+    assert max_principal_sine(outs[0]["evecs"], outs[1]["evecs"], outs[0]["evals"]) < 1e-5
+    assert abs(outs[0]["restarts"] - outs[1]["restarts"]) <= 2
+    if reorth == native.TRL_REORTH_CGS_IFNEEDED:
+        assert outs[1]["kernel_launches"] < outs[0]["kernel_launches"]
+
+
 def test_cfg1_mixed_reaches_fp64_accuracy(cfg1_oracle):
     A, X0, ref = cfg1_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-5)
@@ -129,6 +146,22 @@ def test_smallest_via_shift(oracle):
     assert np.max(np.abs(lam - exact) / np.abs(exact)) < 1e-9
     ref = oracle.solve_csr(A, 4, 8, 64, X0, tol=1e-10, alpha=-1.0, beta=sigma)
     assert np.max(np.abs(out["evals"] - ref["evals"][:8]) / ref["evals"][:8]) < 1e-10
+
+
+@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS1, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_CGS2, native.TRL_REORTH_MGS])
+@pytest.mark.parametrize("batching", [0, 1])
+def test_shifted_small_problem_to_tight_tolerance(reorth, batching):
+    """sigma*I - A with a wide spectrum, 12 restart cycles to 1e-12: every block step carries a
+    large T_ii component, so any reorganisation of the three-term step that weakens the
+    reorthogonalisation shows up as lost orthogonality after the first restart."""
+    A = P.anisotropic3d(9, coef=(1.0, 3.0, 7.0))
+    sigma = A.gershgorin_bound()
+    X0 = P.initial_block(A.n, 4, seed=3)
+    out = native.solve_csr_host(A, X0, bs=4, nev=4, ncv=64, tol=1e-12, alpha=-1.0, beta=sigma, reorth=reorth, batching=batching)
+    assert out["converged"]
+    exact = np.sort(np.linalg.eigvalsh(A.to_dense()))[:4]
+    assert np.max(np.abs(sigma - out["evals"] - exact) / np.abs(exact)) < 1e-9
+    assert np.max(out["resid"]) < 1e-11
 
 
 def test_invalid_parameters_raise():

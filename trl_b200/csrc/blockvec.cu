@@ -425,6 +425,98 @@ __global__ void __launch_bounds__(kThreads) k_block_gemm(const T* in, int64_t is
   }
 }
 
+// ---------------------------------------------------------------- restart rotation
+// W_j = sum_{i<m} V_i Y(i,j) for the output columns [c0, c0 + 8*NTC) of the N = k*BS columns
+// (one chunk of output columns per launch). As a GEMM, out[rows x N] = V[rows x K] * Yhat[K x N]
+// with K = m*BS: 2*n*K*N flops over (K + N)*n elements, ~9 flop/B at the thick restart's
+// shapes, so the kernel is bound by the FP64 DMMA rate rather than by HBM.
+// The chunk of Yhat lives in shared memory in DMMA B-fragment order (for every k-step of 4
+// rows and n-tile of 8 columns the 32 values in lane order: one conflict-free 256-byte load
+// per fragment) and is loaded once per CTA. Each warp owns RT tiles of 8 rows and streams the
+// m input blocks through a register ring D blocks deep, so every load is issued D blocks
+// before the DMMAs that consume it.
+constexpr int kRotThreads = 512;
+
+template <typename T, int BS, int NTC, int RT, int D>
+__global__ void __launch_bounds__(kRotThreads, 1) k_rotate(const T* __restrict__ V, int64_t vstride, int m, const double* __restrict__ Y, int ldy, int N, int c0,
+                                                           T* __restrict__ W, int64_t wstride, int64_t n)
+{
+  constexpr int KSB = BS / 4; // k-steps per input block
+  extern __shared__ double sY[];
+  const int ks_total = m * KSB;
+  for (int idx = threadIdx.x; idx < ks_total * NTC * 32; idx += blockDim.x) {
+    const int ln = idx & 31, f = idx >> 5;
+    const int nt = f % NTC, ks = f / NTC;
+    const int krow = ks * 4 + (ln & 3), col = c0 + nt * 8 + (ln >> 2);
+    double v = 0.0;
+    if (col < N) {
+      const int i = krow / BS, r = krow % BS, j = col / BS, cc = col % BS;
+      v = Y[(static_cast<int64_t>(i) * ldy + j) * (BS * BS) + r * BS + cc];
+    }
+    sY[idx] = v;
+  }
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int64_t warp = static_cast<int64_t>(blockIdx.x) * (kRotThreads / 32) + (threadIdx.x >> 5);
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * (kRotThreads / 32);
+
+  for (int64_t r0 = warp * 8 * RT; r0 < n; r0 += nwarps * 8 * RT) {
+    double acc[RT][NTC][2];
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt)
+#pragma unroll
+      for (int nt = 0; nt < NTC; ++nt) acc[rt][nt][0] = acc[rt][nt][1] = 0.0;
+
+    double a[D][RT][KSB];
+    auto load = [&](double(&dst)[RT][KSB], int blk) {
+#pragma unroll
+      for (int rt = 0; rt < RT; ++rt) {
+        const int64_t row = r0 + rt * 8 + g;
+#pragma unroll
+        for (int ks = 0; ks < KSB; ++ks)
+          dst[rt][ks] = (blk < m && row < n) ? static_cast<double>(V[static_cast<int64_t>(blk) * vstride + row * BS + ks * 4 + t4]) : 0.0;
+      }
+    };
+#pragma unroll
+    for (int d = 0; d < D; ++d) load(a[d], d);
+
+    for (int ib = 0; ib < m; ib += D) {
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int i = ib + d;
+        if (i < m) {
+#pragma unroll
+          for (int ks = 0; ks < KSB; ++ks) {
+            const double* bf = sY + static_cast<size_t>((i * KSB + ks) * NTC) * 32 + lane;
+#pragma unroll
+            for (int nt = 0; nt < NTC; ++nt) {
+              const double b = bf[nt * 32];
+#pragma unroll
+              for (int rt = 0; rt < RT; ++rt) dmma_m8n8k4(acc[rt][nt][0], acc[rt][nt][1], a[d][rt][ks], b);
+            }
+          }
+        }
+        load(a[d], i + D);
+      }
+    }
+
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt) {
+      const int64_t row = r0 + rt * 8 + g;
+      if (row >= n) continue;
+#pragma unroll
+      for (int nt = 0; nt < NTC; ++nt)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = c0 + nt * 8 + 2 * t4 + e;
+          if (col < N) W[static_cast<int64_t>(col / BS) * wstride + row * BS + (col % BS)] = static_cast<T>(acc[rt][nt][e]);
+        }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- update + Gram in one pass
 // out = (accumulate ? out : 0) + sign * sum_{i<MB} in_i Coef(i),  Coef(i) = coef + i*BS*BS,
 // and in the same pass the Gram matrix out^T out of the values as stored (rounded to T):
@@ -886,6 +978,62 @@ int launch_block_gemm(trl_cuda_context* h, const T* in, int MB, const double* co
   return TRL_OK;
 }
 
+
+// Restart rotation through k_rotate: the output columns are processed in chunks of at most 6
+// n-tiles whose Yhat fragments fit in shared memory. Returns -1 (nothing launched) for block
+// sizes below 4 or bases too deep for one k-step column of fragments; the caller then uses
+// k_block_gemm.
+template <typename T, int BS, int NTC>
+int launch_rotate_chunk(trl_cuda_context* h, const T* V, int m, const double* Y, int ldy, int N, int c0, T* W, int64_t n, size_t smem)
+{
+  constexpr int RT = 2;
+  constexpr int D = (BS >= 16) ? 2 : (BS == 8 ? 4 : 8);
+  auto kern = k_rotate<T, BS, NTC, RT, D>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
+    return set_error(h, TRL_ECUDA, "rotation: %zu bytes of shared memory refused", smem);
+  const int64_t tiles = (n + 8 * RT - 1) / (8 * RT);
+  int64_t grid = h->num_sms;
+  const int64_t need = (tiles + kRotThreads / 32 - 1) / (kRotThreads / 32);
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  kern<<<static_cast<unsigned>(grid), kRotThreads, smem, h->stream>>>(V, n * BS, m, Y, ldy, N, c0, W, n * BS, n);
+  return after_launch(h, "rotate");
+}
+
+template <typename T, int BS>
+int launch_rotate(trl_cuda_context* h, const T* V, int m, const double* Y, int ldy, int k, T* W, int64_t n)
+{
+  if constexpr (BS < 4) {
+    return -1;
+  }
+  else {
+    constexpr size_t kSmemMax = 200 * 1024;
+    const size_t frag_bytes = static_cast<size_t>(m) * (BS / 4) * 32 * sizeof(double); // one n-tile column
+    int ntc_max = static_cast<int>(kSmemMax / frag_bytes);
+    if (ntc_max > 6) ntc_max = 6; // beyond 6 n-tiles the accumulators spill at 128 registers
+    if (ntc_max < 1) return -1;
+    const int N = k * BS;
+    const int tiles = (N + 7) / 8;
+    const int passes = (tiles + ntc_max - 1) / ntc_max;
+    const int per = (tiles + passes - 1) / passes;
+    for (int t0 = 0; t0 < tiles; t0 += per) {
+      const int ntc = (tiles - t0) < per ? (tiles - t0) : per;
+      const size_t smem = frag_bytes * ntc;
+      int st = TRL_OK;
+      switch (ntc) {
+      case 1: st = launch_rotate_chunk<T, BS, 1>(h, V, m, Y, ldy, N, t0 * 8, W, n, smem); break;
+      case 2: st = launch_rotate_chunk<T, BS, 2>(h, V, m, Y, ldy, N, t0 * 8, W, n, smem); break;
+      case 3: st = launch_rotate_chunk<T, BS, 3>(h, V, m, Y, ldy, N, t0 * 8, W, n, smem); break;
+      case 4: st = launch_rotate_chunk<T, BS, 4>(h, V, m, Y, ldy, N, t0 * 8, W, n, smem); break;
+      case 5: st = launch_rotate_chunk<T, BS, 5>(h, V, m, Y, ldy, N, t0 * 8, W, n, smem); break;
+      default: st = launch_rotate_chunk<T, BS, 6>(h, V, m, Y, ldy, N, t0 * 8, W, n, smem); break;
+      }
+      if (st) return st;
+    }
+    return TRL_OK;
+  }
+}
+
 } // namespace trl_detail
 
 static int check_common(trl_cuda_context* h, int dtype, int64_t n, int bs)
@@ -964,6 +1112,11 @@ int trl_cuda_bv_mult(trl_cuda_handle h, int dtype, int mode, const void* X, cons
     accumulate = 1;
     sign = -1.0;
     break;
+  case TRL_SUBTRACT_TRANSPOSE:
+    accumulate = 1;
+    sign = -1.0;
+    transpose = 1;
+    break;
   default: return set_error(h, TRL_EINVAL, "bad mult mode %d", mode);
   }
   if (X == Y && accumulate) return set_error(h, TRL_EINVAL, "accumulating mult requires distinct input and output");
@@ -1016,7 +1169,10 @@ int trl_cuda_block_rotate(trl_cuda_handle h, int dtype, const void* V, int m, co
   if (w0 < v1 && v0 < w1) return set_error(h, TRL_EINVAL, "rotation output overlaps its input");
   ProfScope prof(h, PROF_ROTATE, (static_cast<double>(m) + k) * n * bs * es, 2.0 * n * m * k * bs * bs);
   int st = TRL_OK;
-  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = launch_block_gemm<T, BS>(h, static_cast<const T*>(V), m, Y, ldy, 0, static_cast<T*>(W), k, n, 0, 1.0)));
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
+    st = launch_rotate<T, BS>(h, static_cast<const T*>(V), m, Y, ldy, k, static_cast<T*>(W), n);
+    if (st == -1) st = launch_block_gemm<T, BS>(h, static_cast<const T*>(V), m, Y, ldy, 0, static_cast<T*>(W), k, n, 0, 1.0);
+  }));
   return st;
 }
 

@@ -85,6 +85,7 @@ PhaseOut run_phase(const std::shared_ptr<Context>& ctx, const trl_csr* A, const 
   trl::BlockLanczos<EVP, Reorth> lanczos(evp, ep);
   auto V0 = lanczos.initial_block();
   const auto h = ctx->handle();
+  ctx->flush(); // direct ABI calls follow
   ctx->check(trl_cuda_memcpy(h, V0.data_, X0, sizeof(Storage) * static_cast<std::size_t>(A->n) * bs, TRL_D2D), "initial block");
 
   const auto res = lanczos.solve();

@@ -72,22 +72,26 @@ struct SpmmShape {
   static constexpr int LPR = BS / VEC;              // lanes per row: 1..8
   static constexpr int RPW = 32 / LPR;              // rows per warp iteration
   static constexpr int UG = VEC >= 4 ? 4 : 8;       // gathers a lane issues before its FMAs
-  static constexpr int CH = 64;                     // (col, val) pairs staged per warp per chunk
+  static constexpr int CH = RPW * 8 > 64 ? RPW * 8 : 64; // (col, val) pairs staged per warp per chunk
+  static constexpr int PF = CH / 32;                // pairs each lane prefetches
 };
 
 // A warp owns RPW consecutive rows per iteration; within it a group of LPR lanes owns a row
-// and each lane VEC adjacent columns of the block.
-//  1. rowptr of the warp's rows is loaded one iteration ahead (software prefetch);
-//  2. the rows' (col, val) pairs - one contiguous CSR range - are staged in shared memory
-//     with coalesced warp-wide loads, CH pairs at a time;
-//  3. each group walks its row's pairs in the stage and issues UG independent 16-byte X
-//     gathers before the FMAs that consume them.
+// and each lane VEC adjacent columns of the block. The iterations of a warp form a pipeline:
+//  1. rowptr of the warp's rows is loaded two iterations ahead;
+//  2. the first CH (col, val) pairs of the next iteration's rows - one contiguous CSR range -
+//     are loaded into registers (coalesced, PF per lane) while this iteration's gathers run,
+//     and staged in shared memory at the start of the next iteration (ranges longer than CH
+//     continue chunk by chunk, without prefetch);
+//  3. each group walks its row's pairs in the stage and issues UG independent X gathers
+//     (16 bytes per lane) before the FMAs that consume them.
+// So a warp keeps the CSR stream of one iteration and the X gathers of another in flight.
 template <typename T, int BS>
 __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const T* __restrict__ vals,
                                                    const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta)
 {
   using S = SpmmShape<T, BS>;
-  constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH;
+  constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH, PF = S::PF;
   constexpr int WPC = kThreads / 32;
   __shared__ int s_col[WPC][CH];
   __shared__ T s_val[WPC][CH];
@@ -95,37 +99,68 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* 
   const int sub = lane % LPR;
   const int grp = lane / LPR;
   const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * WPC + w;
-  const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * WPC;
+  const int64_t step = static_cast<int64_t>(gridDim.x) * WPC * RPW;
   int64_t rbase = warp_global * RPW;
   if (rbase >= n) return; // whole warp
-  // lane l < RPW holds rowptr[row l], every lane holds the end offset rowptr[row RPW]
-  // (rows past n read rowptr[n]: empty rows)
-  int rp = (lane < RPW) ? __ldg(rowptr + min(rbase + lane, n)) : 0;
-  int rpe = __ldg(rowptr + min(rbase + RPW, n));
+  // rowptr of an iteration: lane l < RPW holds rowptr[row l], every lane the end offset
+  // rowptr[row RPW] (rows past n read rowptr[n]: empty rows); iterations past n are empty
+  auto load_rp = [&](int64_t base, int& rp, int& rpe) {
+    rp = (base < n && lane < RPW) ? __ldg(rowptr + min(base + lane, n)) : 0;
+    rpe = (base < n) ? __ldg(rowptr + min(base + RPW, n)) : 0;
+  };
+  // the first CH pairs of the range [s, e)
+  auto load_pairs = [&](int s, int e, int (&pc)[PF], T (&pv)[PF]) {
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+      const int p = s + q * 32 + lane;
+      if (p < e) {
+        pc[q] = __ldg(colind + p);
+        pv[q] = __ldg(vals + p);
+      }
+    }
+  };
+  int rp0, rpe0, rp1, rpe1;
+  load_rp(rbase, rp0, rpe0);
+  load_rp(rbase + step, rp1, rpe1);
+  int pc[PF];
+  T pv[PF];
+  load_pairs(__shfl_sync(0xffffffffu, rp0, 0), rpe0, pc, pv);
 
-  for (; rbase < n; rbase += warp_stride * RPW) {
-    const int64_t nbase = rbase + warp_stride * RPW;
-    const int rp_next = (nbase < n && lane < RPW) ? __ldg(rowptr + min(nbase + lane, n)) : 0;
-    const int rpe_next = (nbase < n) ? __ldg(rowptr + min(nbase + RPW, n)) : 0;
-    const int s = __shfl_sync(0xffffffffu, rp, 0);
-    const int e = rpe;
-    const int kb = __shfl_sync(0xffffffffu, rp, grp);
-    const int kn = __shfl_sync(0xffffffffu, rp, (grp + 1) & 31);
-    const int ke = (grp + 1 == RPW) ? rpe : kn;
+  for (; rbase < n; rbase += step) {
+    int rp2, rpe2;
+    load_rp(rbase + 2 * step, rp2, rpe2);
+    const int s = __shfl_sync(0xffffffffu, rp0, 0);
+    const int e = rpe0;
+    const int kb = __shfl_sync(0xffffffffu, rp0, grp);
+    const int kn = __shfl_sync(0xffffffffu, rp0, (grp + 1) & 31);
+    const int ke = (grp + 1 == RPW) ? rpe0 : kn;
+    // stage the prefetched first chunk, then prefetch the next iteration's
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+      if (s + q * 32 + lane < e) {
+        s_col[w][q * 32 + lane] = pc[q];
+        s_val[w][q * 32 + lane] = pv[q];
+      }
+    }
+    load_pairs(__shfl_sync(0xffffffffu, rp1, 0), rpe1, pc, pv);
+    __syncwarp();
+
     T acc[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) acc[i] = T(0);
-
     for (int cs = s; cs < e; cs += CH) { // uniform over the warp
+      if (cs != s) { // a range longer than CH: further chunks without prefetch
+        __syncwarp();
 #pragma unroll
-      for (int q = 0; q < CH / 32; ++q) {
-        const int p = cs + q * 32 + lane;
-        if (p < e) {
-          s_col[w][q * 32 + lane] = __ldg(colind + p);
-          s_val[w][q * 32 + lane] = __ldg(vals + p);
+        for (int q = 0; q < PF; ++q) {
+          const int p = cs + q * 32 + lane;
+          if (p < e) {
+            s_col[w][q * 32 + lane] = __ldg(colind + p);
+            s_val[w][q * 32 + lane] = __ldg(vals + p);
+          }
         }
+        __syncwarp();
       }
-      __syncwarp();
       const int lo = max(kb, cs) - cs, hi = min(ke, cs + CH) - cs;
       for (int t = lo; t < hi; t += UG) {
         T x[UG][VEC];
@@ -147,8 +182,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* 
 #pragma unroll
           for (int i = 0; i < VEC; ++i) acc[i] = fma(wv[u], x[u][i], acc[i]);
       }
-      __syncwarp();
     }
+    __syncwarp(); // the stage is rewritten by the next iteration
 
     const int64_t row = rbase + grp;
     if (row < n) {
@@ -165,8 +200,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* 
       }
       store_vec<T, VEC>(Y + row * BS + sub * VEC, y);
     }
-    rp = rp_next;
-    rpe = rpe_next;
+    rp0 = rp1;
+    rpe0 = rpe1;
+    rp1 = rp2;
+    rpe1 = rpe2;
   }
 }
 

@@ -21,7 +21,7 @@ REF_TESTS_BIN = os.path.join(LIB_DIR, "trl_cuda_ref_tests")
 TRL_OK, TRL_EINVAL, TRL_ENOMEM, TRL_ECUDA, TRL_ECHOLESKY, TRL_EEIGEN, TRL_ETIMEOUT, TRL_ENOTSUP = range(8)
 TRL_F64, TRL_F32 = 0, 1
 TRL_H2D, TRL_D2H, TRL_D2D = 0, 1, 2
-TRL_MULT, TRL_MULT_TRANSPOSE, TRL_MULT_ADD, TRL_SUBTRACT = 0, 1, 2, 3
+TRL_MULT, TRL_MULT_TRANSPOSE, TRL_MULT_ADD, TRL_SUBTRACT, TRL_SUBTRACT_TRANSPOSE = 0, 1, 2, 3, 4
 TRL_MODE_FP64, TRL_MODE_FP32, TRL_MODE_MIXED = 0, 1, 2
 TRL_REORTH_MGS, TRL_REORTH_CGS2, TRL_REORTH_CGS_IFNEEDED, TRL_REORTH_CGS1 = 0, 1, 2, 3
 TRL_CGS_ONE, TRL_CGS_TWO, TRL_CGS_IFNEEDED = 0, 1, 2
