@@ -225,6 +225,8 @@ def trl_arm(args, world, rank, local):
     Ah = P.CSRMatrix(A.n, pin(A.rowptr), pin(A.colind), pin(A.values))
     X0h = pin(X0)
     e2e_times, e2e = [], None
+    e2e_clocks = ClockSampler(local)
+    e2e_clocks.start()
     for i in range(1 + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -232,7 +234,9 @@ def trl_arm(args, world, rank, local):
         torch.cuda.synchronize()
         if i > 0:
             e2e_times.append(time.perf_counter() - t0)
+    e2e_clk = e2e_clocks.stop()
     e2e_s = max_over_ranks(statistics.mean(e2e_times))
+    e2e_device_s = e2e["seconds"]  # device time of the last call's solve (its copies excluded)
 
     # ---- roofline of the dominant kernel class (live, over the profiled FP64 solve) ----
     hbm, bf16, src = peaks()
@@ -279,7 +283,8 @@ def trl_arm(args, world, rank, local):
             "kernels_fp32": {"restarts": solve32["restarts"], "seconds": solve32["seconds"], "classes": kern32},
             "roofline": roofline,
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(e2e["h2d_bytes"]), "d2h_bytes_per_step": int(e2e["d2h_bytes"]),
-                    "api": "trl_solve_csr_host (pinned host CSR + start block in, eigenvalues + eigenvectors out)"},
+                    "api": "trl_solve_csr_host (pinned host CSR + start block in, eigenvalues + eigenvectors out)",
+                    "steps_s": e2e_times, "device_s_last": e2e_device_s, "clocks": e2e_clk},
             "gpu_launches": launches // max(1, args.steps) * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
@@ -343,6 +348,8 @@ def profile_case(args):
     spmm    the operator apply on the full workload (CSR 113 MB, X and Y 57 MB each);
     dot / update   one multi-block inner product / projection update against --nblk
             basis blocks of the workload (n x 8 FP64 each);
+    project one Gram-Schmidt pass as the solver issues it (dot + update with the Gram of
+            the result) against --nblk basis blocks;
     rotate  the thick-restart rotation V (48 blocks) x Y -> 5 blocks.
     Every case reads and writes more than the 126 MB L2 and holds at most ~3 GB."""
     import torch
@@ -366,6 +373,11 @@ def profile_case(args):
         Y = torch.empty_like(X)
         for _ in range(args.reps):
             h.spmm(Ad, X, Y)
+    elif args.case == "project":
+        store = torch.randn(args.nblk + 1, A.n, bs, dtype=dt, device="cuda")
+        G = torch.empty(bs, bs, dtype=torch.float64, device="cuda")
+        for _ in range(args.reps):
+            h.project_out(store[: args.nblk], store[args.nblk], native.TRL_CGS_ONE, G)
     elif args.case in ("dot", "update"):
         V = torch.randn(args.nblk, A.n, bs, dtype=dt, device="cuda")
         w = torch.randn(A.n, bs, dtype=dt, device="cuda")
@@ -393,7 +405,7 @@ def main():
     ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
     ap.add_argument("--fp32-tol", type=float, default=1e-5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["solve", "spmm", "dot", "update", "rotate"], default=None,
+    ap.add_argument("--case", choices=["solve", "spmm", "dot", "update", "project", "rotate"], default=None,
                     help="profiling driver: run one piece of the workload and exit (see profile_case)")
     ap.add_argument("--restarts", type=int, default=3)
     ap.add_argument("--nblk", type=int, default=24)

@@ -348,3 +348,25 @@ def test_convert_and_norm1(cuda_handle):
     cuda_handle.convert(y, x)
     torch.cuda.synchronize()
     assert torch.equal(y, x.float())
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+def test_spmm_on_elasticity_and_zipf_patterns(cuda_handle, oracle, bs, dtype):
+    """The structures of the mixed-precision and bandwidth-stress workloads at small size:
+    81 entries per row in 3x3 node blocks (elasticity, 27-point coupling) and heavy-tailed
+    row lengths up to the cap (Zipf(1.5) degrees, mirrored)."""
+    rng = np.random.default_rng(17 * bs)
+    for A in (P.elasticity27(7, seed=3), P.zipf_symmetric(6000, cap=512, seed=4)):
+        X = as_dt(rng.standard_normal((A.n, bs)), dtype)
+        vals = A.values.astype(np.float32).astype(np.float64) if dtype == torch.float32 else A.values
+        Ah = P.CSRMatrix(A.n, A.rowptr, A.colind, vals)
+        ref = oracle.spmm(Ah, X)
+        Ad = native.DeviceCSRTensors.from_host(Ah, dtype)
+        Yd = torch.zeros((A.n, bs), dtype=dtype, device="cuda")
+        cuda_handle.spmm(Ad, dev(X, dtype), Yd)
+        rows = A.row_indices()
+        mag = np.zeros(A.n)
+        np.add.at(mag, rows, np.abs(vals) * np.abs(X[A.colind]).max(axis=1))
+        # FP64 to rounding; FP32 accumulates in FP32 (relative to the summed magnitudes)
+        close(host(Yd), ref, mag.max(), 1e-12 if dtype == torch.float64 else 2e-6)

@@ -164,6 +164,40 @@ def test_shifted_small_problem_to_tight_tolerance(reorth, batching):
     assert np.max(out["resid"]) < 1e-11
 
 
+def test_elasticity_smallest_fp64_and_mixed(oracle):
+    """The mixed-precision workload's matrix family at small size (8^3 nodes x 3 dofs,
+    27-point coupling, diagonal dominance 1.05): 16 smallest eigenpairs through sigma*I - A,
+    FP64 and mixed, against the reference's OpenMP backend and a dense eigensolve."""
+    A = P.elasticity27(8, seed=42)
+    sigma = A.gershgorin_bound()
+    X0 = P.initial_block(A.n, 8, seed=42)
+    ref = oracle.solve_csr(A, 8, 16, 128, X0, tol=1e-10, alpha=-1.0, beta=sigma)
+    assert ref["converged"]
+    exact = np.sort(np.linalg.eigvalsh(A.to_dense()))[:16]
+    for mode in (native.TRL_MODE_FP64, native.TRL_MODE_MIXED):
+        out = native.solve_csr_host(A, X0, bs=8, nev=16, ncv=128, tol=1e-10, alpha=-1.0, beta=sigma, mode=mode, fp32_tol=1e-5)
+        assert out["converged"], mode
+        assert np.max(np.abs(out["evals"] - ref["evals"][:16]) / np.abs(ref["evals"][:16])) < 1e-10, mode
+        assert np.max(np.abs((sigma - out["evals"]) - exact)) < 1e-9 * sigma, mode
+        assert out["max_rel_residual"] < 1e-9, mode
+
+
+@pytest.mark.parametrize("bs", [4, 8, 16])
+def test_zipf_largest_against_reference(oracle, bs):
+    """The bandwidth-stress workload's matrix family at small size (n = 20,000, Zipf(1.5)
+    degrees capped at 512, mirrored N(0,1) values): 16 largest-magnitude eigenpairs for
+    block sizes 4, 8, 16 against the reference's OpenMP backend."""
+    A = P.zipf_symmetric(20_000, seed=7)
+    X0 = P.initial_block(A.n, bs, seed=11)
+    ncv = 16 * bs
+    ref = oracle.solve_csr(A, bs, 16, ncv, X0, tol=1e-10)
+    assert ref["converged"]
+    out = native.solve_csr_host(A, X0, bs=bs, nev=16, ncv=ncv, tol=1e-10)
+    assert out["converged"]
+    assert np.max(np.abs(out["evals"] - ref["evals"][:16]) / np.abs(ref["evals"][:16])) < 1e-10
+    assert out["max_rel_residual"] < 1e-9
+
+
 def test_invalid_parameters_raise():
     A = P.laplace1d(64)
     X0 = P.initial_block(64, 4)

@@ -303,32 +303,36 @@ __global__ void __launch_bounds__(kThreads) k_block_dot_bulk(const T* __restrict
   }
 }
 
-// out[e] = sum_c partial[c][e]: 32 outputs per CTA, 8 slices of the chunk range per output
-// with four independent accumulators each (the loads overlap), combined in a fixed order.
-__global__ void __launch_bounds__(kThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out,
-                                                              const int* __restrict__ cond = nullptr)
+// out[e] = sum_c partial[c][e]: 32 outputs per CTA, 32 slices of the chunk range per output
+// (one warp each) with four independent accumulators each, so that a few hundred partials
+// take two or three dependent load rounds; the slices are combined in a fixed order, so
+// the result does not depend on scheduling.
+constexpr int kRedThreads = 1024;
+__global__ void __launch_bounds__(kRedThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out,
+                                                                 const int* __restrict__ cond = nullptr)
 {
   if (cond && *cond == 0) return;
-  __shared__ double part[8][33];
+  constexpr int SL = kRedThreads / 32;
+  __shared__ double part[SL][33];
   const int o = threadIdx.x & 31, s = threadIdx.x >> 5;
   const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + o;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   if (e < len) {
     int c = s;
-    for (; c + 24 < chunks; c += 32) {
+    for (; c + 3 * SL < chunks; c += 4 * SL) {
       a0 += partial[static_cast<int64_t>(c) * len + e];
-      a1 += partial[static_cast<int64_t>(c + 8) * len + e];
-      a2 += partial[static_cast<int64_t>(c + 16) * len + e];
-      a3 += partial[static_cast<int64_t>(c + 24) * len + e];
+      a1 += partial[static_cast<int64_t>(c + SL) * len + e];
+      a2 += partial[static_cast<int64_t>(c + 2 * SL) * len + e];
+      a3 += partial[static_cast<int64_t>(c + 3 * SL) * len + e];
     }
-    for (; c < chunks; c += 8) a0 += partial[static_cast<int64_t>(c) * len + e];
+    for (; c < chunks; c += SL) a0 += partial[static_cast<int64_t>(c) * len + e];
   }
   part[s][o] = (a0 + a1) + (a2 + a3);
   __syncthreads();
   if (s == 0 && e < len) {
     double t = 0.0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) t += part[q][o];
+    for (int q = 0; q < SL; ++q) t += part[q][o];
     out[e] = t;
   }
 }
@@ -517,6 +521,41 @@ __global__ void __launch_bounds__(kRotThreads, 1) k_rotate(const T* __restrict__
   }
 }
 
+// KS adjacent elements p[0..KS) (p aligned to KS * sizeof(T) when that is 8 or 16 bytes),
+// in as few loads as possible; columns past BS are never requested.
+template <typename T, int KS>
+__device__ __forceinline__ void load_cols(const T* p, T (&v)[KS])
+{
+  if constexpr (sizeof(T) == 8 && KS == 2) {
+    const double2 q = *reinterpret_cast<const double2*>(p);
+    v[0] = q.x;
+    v[1] = q.y;
+  }
+  else if constexpr (sizeof(T) == 8 && KS == 4) {
+    const double2 q0 = *reinterpret_cast<const double2*>(p), q1 = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = q0.x;
+    v[1] = q0.y;
+    v[2] = q1.x;
+    v[3] = q1.y;
+  }
+  else if constexpr (sizeof(T) == 4 && KS == 2) {
+    const float2 q = *reinterpret_cast<const float2*>(p);
+    v[0] = q.x;
+    v[1] = q.y;
+  }
+  else if constexpr (sizeof(T) == 4 && KS == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
+  }
+  else {
+#pragma unroll
+    for (int i = 0; i < KS; ++i) v[i] = p[i];
+  }
+}
+
 // ---------------------------------------------------------------- update + Gram in one pass
 // out = (accumulate ? out : 0) + sign * sum_{i<MB} in_i Coef(i),  Coef(i) = coef + i*BS*BS,
 // and in the same pass the Gram matrix out^T out of the values as stored (rounded to T):
@@ -557,18 +596,19 @@ __global__ void __launch_bounds__(kThreads) k_update_gram(const T* in, int64_t i
         }
     }
     for (int ib0 = 0; ib0 < MB; ib0 += U) {
-      double a[U][RT][KS];
+      // k is permuted so that lane t4 owns the KS adjacent columns t4*KS .. t4*KS+KS-1 of
+      // its row (one vector load); the values stay in the storage type until the DMMA
+      T a[U][RT][KS];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const T* A = in + static_cast<int64_t>(min(ib0 + u, MB - 1)) * istride;
 #pragma unroll
         for (int r = 0; r < RT; ++r) {
           const int64_t row = r0 + r * 8 + g;
+          if (row < n && t4 * KS < BS) load_cols<T, KS>(A + row * BS + t4 * KS, a[u][r]);
+          else
 #pragma unroll
-          for (int ks = 0; ks < KS; ++ks) {
-            const int kcol = ks * 4 + t4;
-            a[u][r][ks] = (row < n && kcol < BS) ? static_cast<double>(A[row * BS + kcol]) : 0.0;
-          }
+            for (int ks = 0; ks < KS; ++ks) a[u][r][ks] = T(0);
         }
       }
 #pragma unroll
@@ -579,10 +619,10 @@ __global__ void __launch_bounds__(kThreads) k_update_gram(const T* in, int64_t i
           for (int ks = 0; ks < KS; ++ks)
 #pragma unroll
             for (int t = 0; t < NT; ++t) {
-              const int krow = ks * 4 + t4, ncol = t * 8 + g;
+              const int krow = t4 * KS + ks, ncol = t * 8 + g;
               const double b = (krow < BS && ncol < BS) ? sign * __ldg(Cb + krow * BS + ncol) : 0.0;
 #pragma unroll
-              for (int r = 0; r < RT; ++r) dmma_m8n8k4(acc[r][t][0], acc[r][t][1], a[u][r][ks], b);
+              for (int r = 0; r < RT; ++r) dmma_m8n8k4(acc[r][t][0], acc[r][t][1], static_cast<double>(a[u][r][ks]), b);
             }
         }
       }
@@ -666,34 +706,44 @@ __global__ void k_select_block(const int* __restrict__ flag, const double* __res
 // the inverse are column-parallel over one warp. A pivot <= 0 (or NaN) records
 // TRL_DEV_CHOLESKY and writes Uinv = I, leaving the apply a no-op.
 template <int BS>
-__global__ void __launch_bounds__(kThreads) k_gram_factor(const double* __restrict__ src, int chunks, double* __restrict__ Uinv, double* __restrict__ R, int first, int* status)
+__global__ void __launch_bounds__(kRedThreads) k_gram_factor(const double* __restrict__ src, int chunks, double* __restrict__ Uinv, double* __restrict__ R, int first,
+                                                             int* status)
 {
+  constexpr int SL = kRedThreads / 32; // slices of the chunk range per output
   __shared__ double G[BS * BS], L[BS][BS + 1], Li[BS][BS + 1], Ro[BS * BS];
-  __shared__ double part[8][32];
+  __shared__ double part[SL][33];
   __shared__ int bad;
   const int tid = threadIdx.x;
-  // 1. G
+  // 1. G (the same fixed-order reduction as k_reduce_partials)
   if (chunks > 0) {
     for (int e0 = 0; e0 < BS * BS; e0 += 32) {
       const int o = tid & 31, s = tid >> 5, e = e0 + o;
-      double a = 0.0;
-      if (e < BS * BS)
-        for (int c = s; c < chunks; c += 8) a += src[static_cast<int64_t>(c) * BS * BS + e];
-      part[s][o] = a;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      if (e < BS * BS) {
+        int c = s;
+        for (; c + 3 * SL < chunks; c += 4 * SL) {
+          a0 += src[static_cast<int64_t>(c) * BS * BS + e];
+          a1 += src[static_cast<int64_t>(c + SL) * BS * BS + e];
+          a2 += src[static_cast<int64_t>(c + 2 * SL) * BS * BS + e];
+          a3 += src[static_cast<int64_t>(c + 3 * SL) * BS * BS + e];
+        }
+        for (; c < chunks; c += SL) a0 += src[static_cast<int64_t>(c) * BS * BS + e];
+      }
+      part[s][o] = (a0 + a1) + (a2 + a3);
       __syncthreads();
       if (s == 0 && e < BS * BS) {
         double t = 0.0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) t += part[q][o];
+        for (int q = 0; q < SL; ++q) t += part[q][o];
         G[e] = t;
       }
       __syncthreads();
     }
   }
   else {
-    for (int e = tid; e < BS * BS; e += kThreads) G[e] = src[e];
+    for (int e = tid; e < BS * BS; e += blockDim.x) G[e] = src[e];
   }
-  for (int e = tid; e < BS * BS; e += kThreads) Ro[e] = R[e];
+  for (int e = tid; e < BS * BS; e += blockDim.x) Ro[e] = R[e];
   if (tid == 0) bad = 0;
   __syncthreads();
   if (tid < 32) {
@@ -752,69 +802,6 @@ __global__ void __launch_bounds__(kThreads) k_gram_factor(const double* __restri
   }
 }
 
-// ---------------------------------------------------------------- small Cholesky
-// G = U^T U (lower triangle of G read, as an LL^T factorisation); writes U^{-1} for the
-// apply and folds U into R (R <- U on the first pass, R <- U R afterwards, so that
-// X_in = X_out R across passes). A pivot <= 0 records TRL_DEV_CHOLESKY and writes the
-// identity so that the apply leaves X unchanged.
-template <int BS>
-__global__ void k_chol_factor(const double* __restrict__ G, double* __restrict__ Uinv, double* __restrict__ R, int first, int* status)
-{
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double L[BS][BS];
-  bool ok = true;
-  for (int j = 0; j < BS && ok; ++j) {
-    double d = G[j * BS + j];
-    for (int k = 0; k < j; ++k) d -= L[j][k] * L[j][k];
-    if (!(d > 0.0)) {
-      ok = false;
-      break;
-    }
-    const double ljj = sqrt(d);
-    L[j][j] = ljj;
-    for (int i = j + 1; i < BS; ++i) {
-      double s = G[i * BS + j];
-      for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
-      L[i][j] = s / ljj;
-    }
-    for (int i = 0; i < j; ++i) L[i][j] = 0.0;
-  }
-  if (!ok) {
-    atomicOr(status, TRL_DEV_CHOLESKY);
-    for (int i = 0; i < BS * BS; ++i) Uinv[i] = (i / BS == i % BS) ? 1.0 : 0.0;
-    return;
-  }
-  // U = L^T; inverse of U by back substitution, column by column
-  double Ui[BS][BS];
-  for (int c = 0; c < BS; ++c) {
-    for (int i = BS - 1; i >= 0; --i) {
-      if (i > c) {
-        Ui[i][c] = 0.0;
-        continue;
-      }
-      double s = (i == c) ? 1.0 : 0.0;
-      for (int k = i + 1; k <= c; ++k) s -= L[k][i] * Ui[k][c]; // U[i][k] = L[k][i]
-      Ui[i][c] = s / L[i][i];
-    }
-  }
-  for (int i = 0; i < BS; ++i)
-    for (int c = 0; c < BS; ++c) Uinv[i * BS + c] = Ui[i][c];
-  if (first) {
-    for (int i = 0; i < BS; ++i)
-      for (int c = 0; c < BS; ++c) R[i * BS + c] = (c >= i) ? L[c][i] : 0.0;
-  }
-  else {
-    double Rn[BS][BS];
-    for (int i = 0; i < BS; ++i)
-      for (int c = 0; c < BS; ++c) {
-        double s = 0.0;
-        for (int k = i; k <= c; ++k) s += L[k][i] * R[k * BS + c];
-        Rn[i][c] = (c >= i) ? s : 0.0;
-      }
-    for (int i = 0; i < BS; ++i)
-      for (int c = 0; c < BS; ++c) R[i * BS + c] = Rn[i][c];
-  }
-}
 
 } // namespace
 
@@ -844,7 +831,7 @@ int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, i
   k_block_dot<T, BS, JC, G><<<grid, kThreads, 0, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -873,7 +860,7 @@ int launch_block_dot_bulk(trl_cuda_context* h, const T* V, int nblk, const T* W,
   k_block_dot_bulk<T, BS, JC, S, TB><<<dim3(gj, static_cast<unsigned>(chunks)), kThreads, smem, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial, h->d_status, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -914,17 +901,21 @@ int launch_update_gram_partials(trl_cuda_context* h, const T* in, int MB, const 
                                 double** partial, int* chunks)
 {
   constexpr int NT = (BS + 7) / 8;
-  constexpr int KS = (BS + 3) / 4;
-  constexpr int RT = NT >= 2 ? 1 : 2;
-  constexpr int U = KS >= 4 ? 2 : 4;
-  const unsigned grid = grid_for(h, (n + 8 * RT - 1) / (8 * RT), kWarps, 4);
+  // Measured on B200 (24 blocks of 884,736 x 8, GB/s of algorithmic bytes; copy peak
+  // 6,539): one input block per loop iteration (U = 1) beats explicit multi-block register
+  // prefetch (U = 4: FP64 6,075, FP32 3,860), and 8-row tiles per warp RT = 4 (FP64, 6,784)
+  // and RT = 2 (FP32, 5,439) with two resident waves of CTAs do best.
+  constexpr int RT = NT >= 2 ? 1 : (sizeof(T) == 8 ? 4 : 2);
+  static int resident = 0;
+  if (resident == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_update_gram<T, BS, RT, 1>, kThreads, 0) != cudaSuccess || resident < 1) resident = 4;
+    cudaGetLastError();
+  }
+  const unsigned grid = grid_for(h, (n + 8 * RT - 1) / (8 * RT), kWarps, 2 * resident);
   *partial = static_cast<double*>(workspace(h, static_cast<size_t>(grid) * BS * BS * sizeof(double)));
   *chunks = static_cast<int>(grid);
   if (!*partial) return TRL_ENOMEM;
-  if (MB == 1) // a single input block: no point loading it U times
-    k_update_gram<T, BS, RT, 1><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
-  else
-    k_update_gram<T, BS, RT, U><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
+  k_update_gram<T, BS, RT, 1><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
   return after_launch(h, "update_gram");
 }
 
@@ -935,7 +926,7 @@ int launch_update_gram(trl_cuda_context* h, const T* in, int MB, const double* c
   int chunks = 0;
   int st = launch_update_gram_partials<T, BS>(h, in, MB, coef, out, n, accumulate, sign, cond, &partial, &chunks);
   if (st) return st;
-  k_reduce_partials<<<(BS * BS + 31) / 32, kThreads, 0, h->stream>>>(partial, chunks, BS * BS, G, cond);
+  k_reduce_partials<<<(BS * BS + 31) / 32, kRedThreads, 0, h->stream>>>(partial, chunks, BS * BS, G, cond);
   return after_launch(h, "update_gram reduce");
 }
 
@@ -1208,7 +1199,7 @@ int trl_cuda_cholqr_gram(trl_cuda_handle h, int dtype, void* X, int64_t n, int b
   int chunks = 0;
   for (int p = 0; p < passes; ++p) {
     int st = TRL_OK;
-    TRL_DISPATCH_BS(bs, k_gram_factor<BS><<<1, kThreads, 0, h->stream>>>(src, chunks, Uinv, R, p == 0, h->d_status));
+    TRL_DISPATCH_BS(bs, k_gram_factor<BS><<<1, kRedThreads, 0, h->stream>>>(src, chunks, Uinv, R, p == 0, h->d_status));
     st = after_launch(h, "cholqr factor");
     if (st) return st;
     if (p + 1 < passes) {
@@ -1372,7 +1363,7 @@ static int noalloc_dot(cudaStream_t stream, int sms, double* partial, const T* V
   // so nothing left in the array by an earlier call is used and nothing needs clearing
   k_block_dot<T, BS, JC, G><<<dim3(gj, static_cast<unsigned>(chunks)), kThreads, 0, stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial);
   if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kThreads, 0, stream>>>(partial, static_cast<int>(chunks), len, C);
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, stream>>>(partial, static_cast<int>(chunks), len, C);
   if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
   return TRL_OK;
 }
