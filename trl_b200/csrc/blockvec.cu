@@ -878,6 +878,10 @@ int launch_block_dot(trl_cuda_context* h, const T* V, int nblk, const T* W, int6
   // algorithmic bytes; the STREAM copy reference is 6,552): FP64 with 2 KB tiles, JC=8, S=3
   // gives 6,662 (24 blocks) and 6,970 (48 blocks); FP32 with 4 KB tiles gives 4,371 (8),
   // 5,269 (24) and with JC=4 5,804 (48).
+  // A single block (the driver's T_ii = V_i^T W, both operands usually still in L2 from the
+  // SpMM): the register-fed kernel with 8 (FP64) / 4 (FP32) row groups per warp and 4 CTAs
+  // per SM measured 6,851 / 5,682 GB/s against 4,759 / 4,562 for the bulk pipeline.
+  if (nblk == 1 && BS <= 8) return launch_block_dot_jc<T, BS, 1, (sizeof(T) == 8 ? 8 : 4)>(h, V, nblk, W, n, C, cond);
   if constexpr ((BS * sizeof(T)) % 16 == 0) {
     constexpr int TBS = (BS * sizeof(T) <= 64) ? 2048 : 4096; // small tiles where 32 rows fit
     constexpr int JCL = BS >= 16 ? 4 : 8;

@@ -2,11 +2,11 @@
 // used by the eigenvalue adjoint.
 //
 // SpMM scheduling: a row is owned by a group of LPR lanes; each lane carries VEC adjacent
-// columns of the block so that one X row is gathered with LPR 16-byte loads. The group
-// reads LPR consecutive (col, val) pairs with one coalesced load per lane and broadcasts
-// them with group-local shuffles, so every X gather is issued without waiting on index
-// loads of the other entries. Accumulation is in the storage type (FP32 for the mixed
-// mode, as the FP32 SpMM is specified; FP64 otherwise).
+// columns of the block so that one X row is gathered with LPR 16-byte loads. A warp's
+// consecutive rows form one contiguous CSR range, staged in shared memory with coalesced
+// loads, so that every X gather is issued without waiting on index loads of the other
+// entries (see k_spmm). Accumulation is in the storage type (FP32 for the mixed mode, as
+// the FP32 SpMM is specified; FP64 otherwise).
 #include "common.cuh"
 
 #include <algorithm>
