@@ -69,26 +69,49 @@ template <typename T, int BS>
 struct SpmmShape {
   static constexpr int max_vec = 16 / static_cast<int>(sizeof(T));
   static constexpr int VEC = max_vec < BS ? max_vec : BS;
-  static constexpr int LPR = BS / VEC;              // lanes per row: 1..8
-  static constexpr int RPW = 32 / LPR;              // rows per warp iteration
-  static constexpr int UG = VEC >= 4 ? 4 : 8;       // gathers a lane issues before its FMAs
+  static constexpr int LPR = BS / VEC;                   // lanes per row: 1..8
+  static constexpr int RPW = 32 / LPR;                   // rows per warp iteration
   static constexpr int CH = RPW * 8 > 64 ? RPW * 8 : 64; // (col, val) pairs staged per warp per chunk
-  static constexpr int PF = CH / 32;                // pairs each lane prefetches
+  static constexpr int PF = CH / 32;                     // pairs each lane stages per chunk
+  // Measured on B200 (96^3 7-point operator, block 8): FP64 4 gathers in flight per lane
+  // and 6 CTAs per SM (40 registers) take 49.6 us against 53.4 us for 8 gathers at 4 CTAs
+  // per SM; FP32 prefers 8 gathers at 4 CTAs per SM (28.8 us). A software prefetch of the
+  // next row group's CSR range, and contiguous row ranges per CTA, measured slower.
+  static constexpr int UG = sizeof(T) == 8 ? 4 : 8;      // gathers a lane issues before its FMAs
+  static constexpr int MINB = sizeof(T) == 8 ? 6 : 4;    // CTAs per SM the registers must allow
 };
 
+// The CSR stream is read once: load it without allocating in L1, which keeps L1 for the
+// X rows that neighbouring rows gather again.
+__device__ __forceinline__ int ld_stream(const int32_t* p)
+{
+  int v;
+  asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p)
+{
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p)
+{
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
 // A warp owns RPW consecutive rows per iteration; within it a group of LPR lanes owns a row
-// and each lane VEC adjacent columns of the block. The iterations of a warp form a pipeline:
-//  1. rowptr of the warp's rows is loaded two iterations ahead;
-//  2. the first CH (col, val) pairs of the next iteration's rows - one contiguous CSR range -
-//     are loaded into registers (coalesced, PF per lane) while this iteration's gathers run,
-//     and staged in shared memory at the start of the next iteration (ranges longer than CH
-//     continue chunk by chunk, without prefetch);
+// and each lane VEC adjacent columns of the block.
+//  1. rowptr of the warp's rows is loaded one iteration ahead;
+//  2. the rows' (col, val) pairs - one contiguous CSR range - are staged in shared memory
+//     with coalesced warp-wide loads, CH pairs at a time;
 //  3. each group walks its row's pairs in the stage and issues UG independent X gathers
 //     (16 bytes per lane) before the FMAs that consume them.
-// So a warp keeps the CSR stream of one iteration and the X gathers of another in flight.
 template <typename T, int BS>
-__global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const T* __restrict__ vals,
-                                                   const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta)
+__global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
+                                                                         const T* __restrict__ vals, const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta)
 {
   using S = SpmmShape<T, BS>;
   constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH, PF = S::PF;
@@ -98,69 +121,40 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int sub = lane % LPR;
   const int grp = lane / LPR;
-  const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * WPC + w;
   const int64_t step = static_cast<int64_t>(gridDim.x) * WPC * RPW;
-  int64_t rbase = warp_global * RPW;
+  int64_t rbase = (static_cast<int64_t>(blockIdx.x) * WPC + w) * RPW;
   if (rbase >= n) return; // whole warp
-  // rowptr of an iteration: lane l < RPW holds rowptr[row l], every lane the end offset
-  // rowptr[row RPW] (rows past n read rowptr[n]: empty rows); iterations past n are empty
+  // lane l < RPW holds rowptr[row l], every lane the end offset rowptr[row RPW] (rows past
+  // n read rowptr[n]: empty rows); iterations past n are empty
   auto load_rp = [&](int64_t base, int& rp, int& rpe) {
     rp = (base < n && lane < RPW) ? __ldg(rowptr + min(base + lane, n)) : 0;
     rpe = (base < n) ? __ldg(rowptr + min(base + RPW, n)) : 0;
   };
-  // the first CH pairs of the range [s, e)
-  auto load_pairs = [&](int s, int e, int (&pc)[PF], T (&pv)[PF]) {
-#pragma unroll
-    for (int q = 0; q < PF; ++q) {
-      const int p = s + q * 32 + lane;
-      if (p < e) {
-        pc[q] = __ldg(colind + p);
-        pv[q] = __ldg(vals + p);
-      }
-    }
-  };
-  int rp0, rpe0, rp1, rpe1;
+  int rp0, rpe0;
   load_rp(rbase, rp0, rpe0);
-  load_rp(rbase + step, rp1, rpe1);
-  int pc[PF];
-  T pv[PF];
-  load_pairs(__shfl_sync(0xffffffffu, rp0, 0), rpe0, pc, pv);
 
   for (; rbase < n; rbase += step) {
-    int rp2, rpe2;
-    load_rp(rbase + 2 * step, rp2, rpe2);
+    int rp1, rpe1;
+    load_rp(rbase + step, rp1, rpe1);
     const int s = __shfl_sync(0xffffffffu, rp0, 0);
     const int e = rpe0;
     const int kb = __shfl_sync(0xffffffffu, rp0, grp);
     const int kn = __shfl_sync(0xffffffffu, rp0, (grp + 1) & 31);
     const int ke = (grp + 1 == RPW) ? rpe0 : kn;
-    // stage the prefetched first chunk, then prefetch the next iteration's
-#pragma unroll
-    for (int q = 0; q < PF; ++q) {
-      if (s + q * 32 + lane < e) {
-        s_col[w][q * 32 + lane] = pc[q];
-        s_val[w][q * 32 + lane] = pv[q];
-      }
-    }
-    load_pairs(__shfl_sync(0xffffffffu, rp1, 0), rpe1, pc, pv);
-    __syncwarp();
-
     T acc[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) acc[i] = T(0);
+
     for (int cs = s; cs < e; cs += CH) { // uniform over the warp
-      if (cs != s) { // a range longer than CH: further chunks without prefetch
-        __syncwarp();
 #pragma unroll
-        for (int q = 0; q < PF; ++q) {
-          const int p = cs + q * 32 + lane;
-          if (p < e) {
-            s_col[w][q * 32 + lane] = __ldg(colind + p);
-            s_val[w][q * 32 + lane] = __ldg(vals + p);
-          }
+      for (int q = 0; q < PF; ++q) {
+        const int p = cs + q * 32 + lane;
+        if (p < e) {
+          s_col[w][q * 32 + lane] = ld_stream(colind + p);
+          s_val[w][q * 32 + lane] = ld_stream(vals + p);
         }
-        __syncwarp();
       }
+      __syncwarp();
       const int lo = max(kb, cs) - cs, hi = min(ke, cs + CH) - cs;
       for (int t = lo; t < hi; t += UG) {
         T x[UG][VEC];
@@ -182,8 +176,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* 
 #pragma unroll
           for (int i = 0; i < VEC; ++i) acc[i] = fma(wv[u], x[u][i], acc[i]);
       }
+      __syncwarp(); // the stage is rewritten by the next chunk or iteration
     }
-    __syncwarp(); // the stage is rewritten by the next iteration
 
     const int64_t row = rbase + grp;
     if (row < n) {
@@ -202,8 +196,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmm(int64_t n, const int32_t* 
     }
     rp0 = rp1;
     rpe0 = rpe1;
-    rp1 = rp2;
-    rpe1 = rpe2;
   }
 }
 
@@ -252,7 +244,7 @@ int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X,
     // one resident wave: every warp strides over the rows (its rowptr prefetch pays off)
     static int resident = 0;
     if (resident == 0) {
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_spmm<T, BS>, kThreads, 0) != cudaSuccess || resident < 1) resident = 4;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_spmm<T, BS>, kThreads, 0) != cudaSuccess || resident < 1) resident = S::MINB;
       cudaGetLastError();
     }
     const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, resident);
