@@ -198,6 +198,16 @@ int trl_cuda_cholqr(trl_cuda_handle h, int dtype, void* X, int64_t n, int bs, in
  * examples/openmp/csrevp.hh:36-44). X and Y must not overlap. */
 int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta);
 
+/* Y = alpha * A X + beta * X + gamma * W (W: n x bs of dtype, may be Y itself, not X): the
+ * three-term step of a Chebyshev filter in one pass. gamma = 0, W = NULL is trl_cuda_spmm.
+ * No counterpart in the reference (used by the mixed-precision refinement). */
+int trl_cuda_spmm3(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta, double gamma, const void* W);
+
+/* Gershgorin interval of alpha*A + beta*I: *host_lo = min_i (c_i - r_i), *host_hi =
+ * max_i (c_i + r_i), c_i = alpha*a_ii + beta, r_i = |alpha| sum_{j != i} |a_ij|. Contains
+ * every eigenvalue. Synchronises the stream. */
+int trl_cuda_csr_gershgorin(trl_cuda_handle h, const trl_csr* A, double alpha, double beta, double* host_lo, double* host_hi);
+
 /* *host_out = max_i sum_j |alpha*a_ij + beta*delta_ij| (= ||alpha*A + beta*I||_1 for a
  * symmetric A; an upper bound of its 2-norm). Synchronises the stream. */
 int trl_cuda_csr_norm1(trl_cuda_handle h, const trl_csr* A, double alpha, double beta, double* host_out);

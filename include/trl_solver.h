@@ -11,9 +11,14 @@
  *   TRL_MODE_FP64   FP64 basis, FP64 SpMM (the plain backend).
  *   TRL_MODE_FP32   FP32 basis and FP32 SpMM; Grams, Cholesky, the projected eigenproblem
  *                   and residuals in FP64. Accuracy is limited by FP32 storage.
- *   TRL_MODE_MIXED  TRL_MODE_FP32 to fp32_tol, then an FP64 refinement: the FP32 Ritz
- *                   vectors are rotated out of the FP32 basis, widened to FP64, and a
- *                   random combination of them starts an FP64 BlockLanczos solve to `tol`.
+ *   TRL_MODE_MIXED  TRL_MODE_FP32 to fp32_tol, then an FP64 refinement of the FP32 phase's
+ *                   kept Ritz vectors (nev/bs + 1 blocks, widened to FP64) to `tol`:
+ *                   TRL_REFINE_CHEBYSHEV (default): Rayleigh-Ritz on those vectors
+ *                     alternated with Chebyshev-filtered subspace iteration on them (the
+ *                     filter damps the spectrum below the kept Ritz values); needs the kept
+ *                     Ritz values on one side of zero, else the Lanczos refinement is used;
+ *                   TRL_REFINE_LANCZOS: a random combination of them starts an FP64
+ *                     BlockLanczos solve.
  *
  * The operator is alpha*A + beta*I (alpha = 1, beta = 0 for A itself).
  * Eigenpairs are returned in the driver's order: decreasing |theta| (evp_base.hh:103).
@@ -31,6 +36,8 @@ enum trl_mode { TRL_MODE_FP64 = 0, TRL_MODE_FP32 = 1, TRL_MODE_MIXED = 2 };
 /* Reorthogonalisation strategy: the reference's ModifiedGS, or the backend's block classical
  * Gram-Schmidt variants (include/trl/impl/cuda/reorthogonalization.hh). */
 enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEEDED = 2, TRL_REORTH_CGS1 = 3 };
+/* FP64 refinement of the mixed mode. */
+enum trl_refine { TRL_REFINE_LANCZOS = 0, TRL_REFINE_CHEBYSHEV = 1 };
 
 typedef struct trl_solve_params {
   int bs;                        /* block size: 1, 2, 4, 8, 16 */
@@ -47,6 +54,7 @@ typedef struct trl_solve_params {
   int want_vectors;              /* form Ritz vectors and true residuals */
   int batching;                  /* fuse the restart rotation (see trl::cuda::Context) */
   unsigned seed;                 /* seed of the refinement's random combination */
+  int refine;                    /* trl_refine (TRL_MODE_MIXED) */
 } trl_solve_params;
 
 typedef struct trl_solve_info {
@@ -63,6 +71,8 @@ typedef struct trl_solve_info {
   double op_norm1;          /* ||op||_1 = max row sum of |alpha*A + beta*I| */
   unsigned long long kernel_launches; /* kernels launched by the backend during the call */
   double h2d_bytes, d2h_bytes;        /* host<->device traffic of the call */
+  unsigned refine_rounds;   /* TRL_REFINE_CHEBYSHEV: Rayleigh-Ritz rounds (0: not used) */
+  unsigned refine_degree;   /* TRL_REFINE_CHEBYSHEV: total filter degree */
 } trl_solve_info;
 
 void trl_solve_params_default(trl_solve_params* p);

@@ -113,6 +113,36 @@ def test_cfg1_mixed_reaches_fp64_accuracy(cfg1_oracle):
     assert out["restarts_fp32"] > 0
 
 
+@pytest.mark.parametrize("refine", [native.TRL_REFINE_CHEBYSHEV, native.TRL_REFINE_LANCZOS])
+def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine):
+    """Both FP64 refinements of the mixed mode from the FP32 phase's kept Ritz vectors: the
+    Chebyshev-filtered subspace iteration with Rayleigh-Ritz, and a BlockLanczos restart."""
+    A, X0, ref = cfg1_oracle
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4, refine=refine)
+    assert out["converged"]
+    exact = P.laplace2d_eigenvalues(128)[:10]
+    assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-11
+    assert np.max(np.abs(out["evals"] - ref["evals"][:10]) / ref["evals"][:10]) < 1e-11
+    assert out["max_theta_residual"] < 1e-10
+    assert max_principal_sine(out["evecs"], ref["ritz"], out["evals"]) < 1e-5
+    if refine == native.TRL_REFINE_CHEBYSHEV:
+        assert out["refine_rounds"] >= 1 and out["refine_degree"] > 0 and out["restarts"] == 0
+    else:
+        assert out["refine_rounds"] == 0 and out["restarts"] > 0
+
+
+def test_mixed_with_kept_values_on_both_sides_of_zero_uses_lanczos(oracle):
+    """Largest-magnitude eigenvalues of an indefinite matrix: the kept Ritz values straddle
+    zero, no one-sided filter applies, and the refinement falls back to BlockLanczos."""
+    A = P.zipf_symmetric(20_000, seed=7)
+    X0 = P.initial_block(A.n, 8, seed=11)
+    ref = oracle.solve_csr(A, 8, 16, 128, X0, tol=1e-10)
+    out = native.solve_csr_host(A, X0, bs=8, nev=16, ncv=128, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4)
+    assert out["converged"]
+    assert out["refine_rounds"] == 0 and out["restarts"] > 0
+    assert np.max(np.abs(out["evals"] - ref["evals"][:16]) / np.abs(ref["evals"][:16])) < 1e-10
+
+
 def test_fp32_mode_accuracy_is_stated(cfg1_oracle):
     A, X0, ref = cfg1_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-5, mode=native.TRL_MODE_FP32)

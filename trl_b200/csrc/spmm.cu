@@ -111,7 +111,8 @@ __device__ __forceinline__ float ld_stream(const float* p)
 //     (16 bytes per lane) before the FMAs that consume them.
 template <typename T, int BS>
 __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
-                                                                         const T* __restrict__ vals, const T* __restrict__ X, T* __restrict__ Y, T alpha, T beta)
+                                                                         const T* __restrict__ vals, const T* __restrict__ X, T* Y, T alpha, T beta, T gamma,
+                                                                         const T* W)
 {
   using S = SpmmShape<T, BS>;
   constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH, PF = S::PF;
@@ -192,6 +193,13 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
 #pragma unroll
         for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i];
       }
+      if (W) { // W may be Y itself: this lane reads its values before it writes them
+        T wv[VEC];
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) wv[i] = W[row * BS + sub * VEC + i];
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) y[i] += gamma * wv[i];
+      }
       store_vec<T, VEC>(Y + row * BS + sub * VEC, y);
     }
     rp0 = rp1;
@@ -224,20 +232,19 @@ using namespace trl_detail;
 
 extern "C" {
 
-int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta)
+static int spmm_impl(trl_cuda_context* h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta, double gamma, const void* W)
 {
-  TRL_CHECK_HANDLE(h);
   if (!A || !X || !Y) return set_error(h, TRL_EINVAL, "null pointer");
   if (!valid_dtype(dtype) || A->value_dtype != dtype) return set_error(h, TRL_ENOTSUP, "SpMM needs CSR values and block in the same dtype (got %d and %d)", A->value_dtype, dtype);
   if (!valid_bs(bs)) return set_error(h, TRL_ENOTSUP, "unsupported block size %d", bs);
   if (A->n < 0 || A->nnz < 0 || A->nnz >= (int64_t(1) << 31)) return set_error(h, TRL_EINVAL, "bad CSR sizes");
   if (A->n == 0) return TRL_OK;
   if (!A->rowptr || (A->nnz > 0 && (!A->colind || !A->values))) return set_error(h, TRL_EINVAL, "null CSR array");
-  if (X == Y) return set_error(h, TRL_EINVAL, "SpMM input and output must not alias");
+  if (X == Y || (W && W == X)) return set_error(h, TRL_EINVAL, "SpMM input must alias neither output nor third operand");
   const size_t es = dtype == TRL_F64 ? 8 : 4;
   if (((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) % (es * bs < 16 ? es * bs : 16)) != 0)
     return set_error(h, TRL_EINVAL, "block vectors must be aligned to min(16, bs*elem) bytes");
-  ProfScope prof(h, PROF_SPMM, A->nnz * (es + 4.0) + 4.0 * (A->n + 1) + 2.0 * A->n * bs * es, 2.0 * A->nnz * bs);
+  ProfScope prof(h, PROF_SPMM, A->nnz * (es + 4.0) + 4.0 * (A->n + 1) + (W ? 3.0 : 2.0) * A->n * bs * es, 2.0 * A->nnz * bs);
   int st = TRL_OK;
   TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
     using S = SpmmShape<T, BS>;
@@ -249,10 +256,22 @@ int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X,
     }
     const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, resident);
     k_spmm<T, BS><<<grid, kThreads, 0, h->stream>>>(A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
-                                                    static_cast<T>(alpha), static_cast<T>(beta));
+                                                    static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma), static_cast<const T*>(W));
     st = after_launch(h, "spmm");
   }));
   return st;
+}
+
+int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta)
+{
+  TRL_CHECK_HANDLE(h);
+  return spmm_impl(h, A, dtype, X, Y, bs, alpha, beta, 0.0, nullptr);
+}
+
+int trl_cuda_spmm3(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta, double gamma, const void* W)
+{
+  TRL_CHECK_HANDLE(h);
+  return spmm_impl(h, A, dtype, X, Y, bs, alpha, beta, gamma, W);
 }
 
 int trl_cuda_sddmm(trl_cuda_handle h, const trl_csr* P, const double* X, int k, const double* w, double* out)
@@ -336,7 +355,61 @@ __global__ void __launch_bounds__(256) k_norm1(int64_t n, const int32_t* __restr
   if ((threadIdx.x & 31) == 0) atomicMax(out, static_cast<unsigned long long>(__double_as_longlong(best)));
 }
 
+// Monotone map of doubles onto unsigned 64-bit integers (for atomicMin/atomicMax).
+__device__ __forceinline__ unsigned long long ordered_bits(double x)
+{
+  const unsigned long long u = static_cast<unsigned long long>(__double_as_longlong(x));
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+// Gershgorin interval of alpha*A + beta*I: [min_i (c_i - r_i), max_i (c_i + r_i)] with
+// c_i = alpha*a_ii + beta and r_i = |alpha| * sum_{j != i} |a_ij|.
+__global__ void __launch_bounds__(256) k_gershgorin(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const void* __restrict__ vals,
+                                                    int f64, double alpha, double beta, unsigned long long* __restrict__ lo_hi)
+{
+  double lo = INFINITY, hi = -INFINITY;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double c = beta, rad = 0.0;
+    for (int p = rowptr[r]; p < rowptr[r + 1]; ++p) {
+      const double a = f64 ? static_cast<const double*>(vals)[p] : static_cast<double>(static_cast<const float*>(vals)[p]);
+      if (colind[p] == r) c += alpha * a;
+      else rad += fabs(alpha * a);
+    }
+    lo = fmin(lo, c - rad);
+    hi = fmax(hi, c + rad);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&lo_hi[0], ordered_bits(lo));
+    atomicMax(&lo_hi[1], ordered_bits(hi));
+  }
+}
+
 } // namespace
+
+extern "C" int trl_cuda_csr_gershgorin(trl_cuda_handle h, const trl_csr* A, double alpha, double beta, double* host_lo, double* host_hi)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!A || !host_lo || !host_hi) return set_error(h, TRL_EINVAL, "null pointer");
+  *host_lo = *host_hi = beta;
+  if (A->n == 0) return TRL_OK;
+  unsigned long long* d = static_cast<unsigned long long*>(workspace(h, 64));
+  if (!d) return TRL_ENOMEM;
+  const unsigned long long init[2] = {~0ull, 0ull};
+  if (int st = trl_cuda_memcpy(h, d, init, sizeof init, TRL_H2D)) return st;
+  k_gershgorin<<<grid_for(h, A->n, 256, 8), 256, 0, h->stream>>>(A->n, A->rowptr, A->colind, A->values, A->value_dtype == TRL_F64, alpha, beta, d);
+  if (int st = after_launch(h, "csr_gershgorin")) return st;
+  unsigned long long bits[2] = {0, 0};
+  if (int st = trl_cuda_memcpy(h, bits, d, sizeof bits, TRL_D2H)) return st;
+  for (int i = 0; i < 2; ++i) {
+    const unsigned long long u = (bits[i] >> 63) ? (bits[i] & 0x7fffffffffffffffull) : ~bits[i];
+    std::memcpy(i == 0 ? host_lo : host_hi, &u, sizeof u);
+  }
+  return TRL_OK;
+}
 
 extern "C" int trl_cuda_csr_norm1(trl_cuda_handle h, const trl_csr* A, double alpha, double beta, double* host_out)
 {

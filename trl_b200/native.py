@@ -25,6 +25,7 @@ TRL_MULT, TRL_MULT_TRANSPOSE, TRL_MULT_ADD, TRL_SUBTRACT, TRL_SUBTRACT_TRANSPOSE
 TRL_MODE_FP64, TRL_MODE_FP32, TRL_MODE_MIXED = 0, 1, 2
 TRL_REORTH_MGS, TRL_REORTH_CGS2, TRL_REORTH_CGS_IFNEEDED, TRL_REORTH_CGS1 = 0, 1, 2, 3
 TRL_CGS_ONE, TRL_CGS_TWO, TRL_CGS_IFNEEDED = 0, 1, 2
+TRL_REFINE_LANCZOS, TRL_REFINE_CHEBYSHEV = 0, 1
 
 P = C.c_void_p
 I64 = C.c_int64
@@ -57,6 +58,8 @@ CUDA_SYMBOLS = {
     "trl_cuda_project_out": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, C.c_int, C.c_double, P]),
     "trl_cuda_spmm": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double]),
     "trl_cuda_csr_norm1": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "trl_cuda_spmm3": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double, C.c_double, P]),
+    "trl_cuda_csr_gershgorin": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "trl_cuda_sddmm": (C.c_int, [P, P, P, C.c_int, P, P]),
     "trl_cuda_eigen_adjoint": (C.c_int, [P, P, P, C.c_int, P, P, C.c_double, C.c_int, P]),
     "trl_cuda_mb_copy": (C.c_int, [P, P, P, C.c_int, C.c_int]),
@@ -83,14 +86,15 @@ class trl_solve_params(C.Structure):
     _fields_ = [("bs", C.c_int), ("mode", C.c_int), ("nev", C.c_uint), ("ncv", C.c_uint), ("max_restarts", C.c_uint),
                 ("tol", C.c_double), ("alpha", C.c_double), ("beta", C.c_double), ("reorth", C.c_int),
                 ("cholqr_passes", C.c_int), ("fp32_tol", C.c_double), ("refine_max_restarts", C.c_uint),
-                ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint)]
+                ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint), ("refine", C.c_int)]
 
 
 class trl_solve_info(C.Structure):
     _fields_ = [("converged", C.c_int), ("restarts", C.c_uint), ("n_op_apply", C.c_uint), ("restarts_fp32", C.c_uint),
                 ("n_op_apply_fp32", C.c_uint), ("seconds", C.c_double), ("seconds_fp32", C.c_double),
                 ("seconds_vectors", C.c_double), ("max_rel_residual", C.c_double), ("max_theta_residual", C.c_double),
-                ("op_norm1", C.c_double), ("kernel_launches", C.c_ulonglong), ("h2d_bytes", C.c_double), ("d2h_bytes", C.c_double)]
+                ("op_norm1", C.c_double), ("kernel_launches", C.c_ulonglong), ("h2d_bytes", C.c_double), ("d2h_bytes", C.c_double),
+                ("refine_rounds", C.c_uint), ("refine_degree", C.c_uint)]
 
 
 SOLVER_SYMBOLS = {
@@ -242,6 +246,15 @@ class Handle:
     def spmm(self, A: "DeviceCSRTensors", X, Y, alpha: float = 1.0, beta: float = 0.0):
         n, bs = X.shape
         self.check(self.lib.trl_cuda_spmm(self.h, C.byref(A.desc), _dtype(X), _ptr(X), _ptr(Y), bs, alpha, beta))
+
+    def spmm3(self, A: "DeviceCSRTensors", X, Y, alpha: float, beta: float, gamma: float, W):
+        n, bs = X.shape
+        self.check(self.lib.trl_cuda_spmm3(self.h, C.byref(A.desc), _dtype(X), _ptr(X), _ptr(Y), bs, alpha, beta, gamma, _ptr(W)))
+
+    def csr_gershgorin(self, A: "DeviceCSRTensors", alpha: float = 1.0, beta: float = 0.0):
+        lo, hi = C.c_double(0.0), C.c_double(0.0)
+        self.check(self.lib.trl_cuda_csr_gershgorin(self.h, C.byref(A.desc), alpha, beta, C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value
 
     def csr_norm1(self, A: "DeviceCSRTensors", alpha: float = 1.0, beta: float = 0.0) -> float:
         out = C.c_double(0.0)
