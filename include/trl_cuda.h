@@ -203,6 +203,11 @@ int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X,
  * No counterpart in the reference (used by the mixed-precision refinement). */
 int trl_cuda_spmm3(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta, double gamma, const void* W);
 
+/* trl_cuda_spmm3 on nb blocks at once: X, Y and W (or W = NULL) each hold nb consecutive
+ * n x bs blocks; block j gets Y_j = alpha A X_j + beta X_j + gamma W_j. Each row group's CSR
+ * entries are read once for all nb blocks. */
+int trl_cuda_spmm_blocks(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, int nb, double alpha, double beta, double gamma, const void* W);
+
 /* Gershgorin interval of alpha*A + beta*I: *host_lo = min_i (c_i - r_i), *host_hi =
  * max_i (c_i + r_i), c_i = alpha*a_ii + beta, r_i = |alpha| sum_{j != i} |a_ij|. Contains
  * every eigenvalue. Synchronises the stream. */

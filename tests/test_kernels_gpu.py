@@ -370,3 +370,70 @@ def test_spmm_on_elasticity_and_zipf_patterns(cuda_handle, oracle, bs, dtype):
         np.add.at(mag, rows, np.abs(vals) * np.abs(X[A.colind]).max(axis=1))
         # FP64 to rounding; FP32 accumulates in FP32 (relative to the summed magnitudes)
         close(host(Yd), ref, mag.max(), 1e-12 if dtype == torch.float64 else 2e-6)
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+@pytest.mark.parametrize("nb", [1, 3, 5])
+def test_spmm_blocks_three_term(cuda_handle, oracle, bs, dtype, nb):
+    """Y_j = alpha A X_j + beta X_j + gamma W_j on nb blocks in one call, with W = Y (the
+    Chebyshev filter's in-place recurrence), W separate and W absent. Short rows stage each
+    warp's CSR range once for all blocks; long rows (Zipf degrees) take the chunked path."""
+    rng = np.random.default_rng(31 * bs + nb)
+    tol = 1e-12 if dtype == torch.float64 else 2e-6
+    for A in (P.anisotropic3d(9), P.zipf_symmetric(4000, cap=400, seed=9)):
+        vals = A.values.astype(np.float32).astype(np.float64) if dtype == torch.float32 else A.values
+        Ah = P.CSRMatrix(A.n, A.rowptr, A.colind, vals)
+        Ad = native.DeviceCSRTensors.from_host(Ah, dtype)
+        X = as_dt(rng.standard_normal((nb, A.n, bs)), dtype)
+        W = as_dt(rng.standard_normal((nb, A.n, bs)), dtype)
+        alpha, beta, gamma = 0.75, -1.25, 0.5
+        ref = np.stack([oracle.spmm(Ah, X[j], alpha, beta) for j in range(nb)])
+        rows = A.row_indices()
+        mag = np.zeros(A.n)
+        np.add.at(mag, rows, np.abs(vals) * np.abs(X).max(axis=(0, 2))[A.colind])
+        scale = abs(alpha) * mag.max() + abs(beta) * np.abs(X).max() + abs(gamma) * np.abs(W).max()
+        Xd = dev(X, dtype)
+        # W separate
+        Yd = torch.full((nb, A.n, bs), float("nan"), dtype=dtype, device="cuda")
+        cuda_handle.spmm_blocks(Ad, Xd, Yd, alpha, beta, gamma, dev(W, dtype))
+        close(host(Yd), ref + gamma * W, scale, tol)
+        # W = Y, updated in place
+        Yd = dev(W, dtype)
+        cuda_handle.spmm_blocks(Ad, Xd, Yd, alpha, beta, gamma, Yd)
+        close(host(Yd), ref + gamma * W, scale, tol)
+        # no W: matches the one-block entry point block by block
+        Yd = torch.full((nb, A.n, bs), float("nan"), dtype=dtype, device="cuda")
+        cuda_handle.spmm_blocks(Ad, Xd, Yd, alpha, beta, 0.0, None)
+        for j in range(nb):
+            Y1 = torch.empty((A.n, bs), dtype=dtype, device="cuda")
+            cuda_handle.spmm3(Ad, Xd[j], Y1, alpha, beta, 0.0, None)
+            assert torch.equal(Yd[j], Y1)
+        close(host(Yd), ref, scale, tol)
+
+
+def test_spmm_blocks_rejects_bad_block_count(cuda_handle):
+    A = native.DeviceCSRTensors.from_host(P.laplace1d(16))
+    X = torch.zeros((0, 16, 4), dtype=torch.float64, device="cuda")
+    with pytest.raises(native.TrlError) as e:
+        cuda_handle.spmm_blocks(A, X, X, 1.0, 0.0, 0.0, None)
+    assert e.value.status == native.TRL_EINVAL
+
+
+@pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-1.0, 40.0), (2.5, -3.0)])
+def test_csr_gershgorin_interval(cuda_handle, alpha, beta):
+    rng = np.random.default_rng(3)
+    for A in (P.anisotropic3d(6), _random_csr(2003, rng)):
+        D = alpha * A.to_dense() + beta * np.eye(A.n)
+        c = np.diag(D)
+        r = np.abs(D).sum(axis=1) - np.abs(c)
+        for dtype in DT:
+            vals = A.values.astype(np.float32).astype(np.float64) if dtype == torch.float32 else A.values
+            Ad = native.DeviceCSRTensors.from_host(P.CSRMatrix(A.n, A.rowptr, A.colind, vals), dtype)
+            lo, hi = cuda_handle.csr_gershgorin(Ad, alpha, beta)
+            if dtype == torch.float64:
+                assert lo == pytest.approx((c - r).min(), rel=1e-13, abs=1e-13)
+                assert hi == pytest.approx((c + r).max(), rel=1e-13, abs=1e-13)
+            ev = np.linalg.eigvalsh(alpha * P.CSRMatrix(A.n, A.rowptr, A.colind, vals).to_dense() + beta * np.eye(A.n)) if A.n < 600 else None
+            if ev is not None:
+                assert lo <= ev.min() + 1e-9 and hi >= ev.max() - 1e-9

@@ -137,13 +137,13 @@ PhaseOut run_phase_r(const std::shared_ptr<Context>& ctx, const trl_csr* A, cons
 // smallest kept Ritz value) amplifies an eigenvector with eigenvalue x > b by
 // T_d((x - c) / e) (c, e the interval's centre and half-width) relative to the damped ones.
 // The filter is applied with the three-term recurrence in the scaled form of Zhou & Saad
-// (2007, "Chebyshev-filtered subspace iteration"), one SpMM per block and degree; the block
-// is re-orthonormalised whenever the spread of amplifications across the kept vectors
-// reaches about 1e6, and a Rayleigh-Ritz step (dense kr*bs eigenproblem) follows every
-// filter round. The Ritz pairs are final when every wanted pair has
+// (2007, "Chebyshev-filtered subspace iteration"), one multi-block SpMM per degree that
+// reads the CSR stream once for all kept blocks; the block is re-orthonormalised whenever
+// the spread of amplifications across the kept vectors reaches about 1e6, and a
+// Rayleigh-Ritz step (dense kr*bs eigenproblem) follows every filter round. The Ritz pairs are final when every wanted pair has
 // ||op x - theta x|| / |theta| < tol (the driver's convergence test, evp_base.hh:128-147).
 // No Krylov basis is built, so there is no reorthogonalisation against a growing basis:
-// each degree costs kr SpMMs of the kept block.
+// each degree costs one CSR pass plus the kr blocks' gathers and stores.
 
 struct RefineOut {
   bool applicable = false; // false: the kept Ritz values straddle zero (use the Lanczos refinement)
@@ -276,7 +276,7 @@ private:
     double* AX = static_cast<double*>(AX_.get());
     double* T = static_cast<double*>(T_.get());
     double* C = static_cast<double*>(C_.get());
-    for (unsigned j = 0; j < kr_; ++j) ctx_->check(trl_cuda_spmm(h_, A_, TRL_F64, blockp(X, j), blockp(AX, j), bs, p_.alpha, p_.beta), "refine Rayleigh-Ritz");
+    ctx_->check(trl_cuda_spmm_blocks(h_, A_, TRL_F64, X, AX, bs, static_cast<int>(kr_), p_.alpha, p_.beta, 0.0, nullptr), "refine Rayleigh-Ritz");
     // lower block triangle of H: column j = X^T (op X_j), blocks k >= j
     for (unsigned j = 0; j < kr_; ++j) {
       ctx_->check(trl_cuda_block_dot(h_, TRL_F64, X, static_cast<int>(kr_), blockp(AX, j), n_, bs, C), "refine Rayleigh-Ritz");
@@ -332,17 +332,14 @@ private:
     double sigma = e / (top - c);
     const double tau = 2.0 / sigma;
     // Y1 = (s op - c) X * sigma / e
-    for (unsigned j = 0; j < kr_; ++j)
-      ctx_->check(trl_cuda_spmm3(h_, A_, TRL_F64, blockp(X, j), blockp(Y, j), bs, al * sigma / e, be * sigma / e, 0.0, nullptr), "refine filter");
+    ctx_->check(trl_cuda_spmm_blocks(h_, A_, TRL_F64, X, Y, bs, static_cast<int>(kr_), al * sigma / e, be * sigma / e, 0.0, nullptr), "refine filter");
     double* prev = X;
     double* curv = Y;
     for (unsigned i = 2; i <= L; ++i) {
       const double sigma2 = 1.0 / (tau - sigma);
       // Y_{i} = 2 sigma2 / e (s op - c) Y_{i-1} - sigma sigma2 Y_{i-2}, written over Y_{i-2}
-      for (unsigned j = 0; j < kr_; ++j)
-        ctx_->check(trl_cuda_spmm3(h_, A_, TRL_F64, blockp(curv, j), blockp(prev, j), bs, 2.0 * sigma2 / e * al, 2.0 * sigma2 / e * be, -sigma * sigma2,
-                                   blockp(prev, j)),
-                    "refine filter");
+      ctx_->check(trl_cuda_spmm_blocks(h_, A_, TRL_F64, curv, prev, bs, static_cast<int>(kr_), 2.0 * sigma2 / e * al, 2.0 * sigma2 / e * be, -sigma * sigma2, prev),
+                  "refine filter");
       std::swap(prev, curv);
       sigma = sigma2;
     }

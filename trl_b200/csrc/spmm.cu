@@ -109,10 +109,11 @@ __device__ __forceinline__ float ld_stream(const float* p)
 //     with coalesced warp-wide loads, CH pairs at a time;
 //  3. each group walks its row's pairs in the stage and issues UG independent X gathers
 //     (16 bytes per lane) before the FMAs that consume them.
-template <typename T, int BS>
+//  With MB (several blocks), a range that fits one stage is staged once for all blocks.
+template <typename T, int BS, bool MB>
 __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
                                                                          const T* __restrict__ vals, const T* __restrict__ X, T* Y, T alpha, T beta, T gamma,
-                                                                         const T* W)
+                                                                         const T* W, int nb, int64_t bstride)
 {
   using S = SpmmShape<T, BS>;
   constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH, PF = S::PF;
@@ -142,11 +143,11 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
     const int kb = __shfl_sync(0xffffffffu, rp0, grp);
     const int kn = __shfl_sync(0xffffffffu, rp0, (grp + 1) & 31);
     const int ke = (grp + 1 == RPW) ? rpe0 : kn;
-    T acc[VEC];
-#pragma unroll
-    for (int i = 0; i < VEC; ++i) acc[i] = T(0);
-
-    for (int cs = s; cs < e; cs += CH) { // uniform over the warp
+    // The CSR range is staged once when it fits the stage and then applied to every block
+    // (X, Y, W hold nb blocks bstride elements apart); longer ranges are staged chunk by
+    // chunk for each block.
+    const bool one_chunk = MB && (e - s) <= CH; // uniform over the warp
+    auto stage = [&](int cs) {
 #pragma unroll
       for (int q = 0; q < PF; ++q) {
         const int p = cs + q * 32 + lane;
@@ -156,52 +157,65 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
         }
       }
       __syncwarp();
-      const int lo = max(kb, cs) - cs, hi = min(ke, cs + CH) - cs;
-      for (int t = lo; t < hi; t += UG) {
-        T x[UG][VEC];
-        T wv[UG];
+    };
+    if (one_chunk) stage(s);
+    for (int b = 0; b < (MB ? nb : 1); ++b) {
+      const T* Xb = X + static_cast<int64_t>(b) * bstride;
+      T acc[VEC];
 #pragma unroll
-        for (int u = 0; u < UG; ++u) {
-          if (t + u < hi) {
-            wv[u] = s_val[w][t + u];
-            load_vec<T, VEC>(X + static_cast<int64_t>(s_col[w][t + u]) * BS + sub * VEC, x[u]);
-          }
-          else {
-            wv[u] = T(0);
+      for (int i = 0; i < VEC; ++i) acc[i] = T(0);
+      for (int cs = s; cs < e; cs += CH) {
+        if (!one_chunk) stage(cs);
+        const int lo = max(kb, cs) - cs, hi = min(ke, cs + CH) - cs;
+        for (int t = lo; t < hi; t += UG) {
+          T x[UG][VEC];
+          T wv[UG];
 #pragma unroll
-            for (int i = 0; i < VEC; ++i) x[u][i] = T(0);
+          for (int u = 0; u < UG; ++u) {
+            if (t + u < hi) {
+              wv[u] = s_val[w][t + u];
+              load_vec<T, VEC>(Xb + static_cast<int64_t>(s_col[w][t + u]) * BS + sub * VEC, x[u]);
+            }
+            else {
+              wv[u] = T(0);
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) x[u][i] = T(0);
+            }
           }
+#pragma unroll
+          for (int u = 0; u < UG; ++u)
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) acc[i] = fma(wv[u], x[u][i], acc[i]);
         }
-#pragma unroll
-        for (int u = 0; u < UG; ++u)
-#pragma unroll
-          for (int i = 0; i < VEC; ++i) acc[i] = fma(wv[u], x[u][i], acc[i]);
+        if (!one_chunk) __syncwarp(); // the stage is rewritten by the next chunk
       }
-      __syncwarp(); // the stage is rewritten by the next chunk or iteration
-    }
 
-    const int64_t row = rbase + grp;
-    if (row < n) {
-      T y[VEC];
-      if (beta != T(0)) {
-        T x[VEC];
-        load_vec<T, VEC>(X + row * BS + sub * VEC, x);
+      const int64_t row = rbase + grp;
+      if (row < n) {
+        T* Yb = Y + static_cast<int64_t>(b) * bstride;
+        T y[VEC];
+        if (beta != T(0)) {
+          T x[VEC];
+          load_vec<T, VEC>(Xb + row * BS + sub * VEC, x);
 #pragma unroll
-        for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i] + beta * x[i];
+          for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i] + beta * x[i];
+        }
+        else {
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i];
+        }
+        if (W) { // W may be Y itself: this lane reads its values before it writes them
+          const T* Wb = W + static_cast<int64_t>(b) * bstride;
+          T wv[VEC];
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) wv[i] = Wb[row * BS + sub * VEC + i];
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) y[i] += gamma * wv[i];
+        }
+        store_vec<T, VEC>(Yb + row * BS + sub * VEC, y);
       }
-      else {
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i];
-      }
-      if (W) { // W may be Y itself: this lane reads its values before it writes them
-        T wv[VEC];
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) wv[i] = W[row * BS + sub * VEC + i];
-#pragma unroll
-        for (int i = 0; i < VEC; ++i) y[i] += gamma * wv[i];
-      }
-      store_vec<T, VEC>(Y + row * BS + sub * VEC, y);
     }
+    if (one_chunk) __syncwarp(); // the stage is rewritten by the next iteration
     rp0 = rp1;
     rpe0 = rpe1;
   }
@@ -232,31 +246,43 @@ using namespace trl_detail;
 
 extern "C" {
 
-static int spmm_impl(trl_cuda_context* h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta, double gamma, const void* W)
+static int spmm_impl(trl_cuda_context* h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, int nb, double alpha, double beta, double gamma,
+                     const void* W)
 {
+  if (nb < 1) return set_error(h, TRL_EINVAL, "block count %d", nb);
   if (!A || !X || !Y) return set_error(h, TRL_EINVAL, "null pointer");
   if (!valid_dtype(dtype) || A->value_dtype != dtype) return set_error(h, TRL_ENOTSUP, "SpMM needs CSR values and block in the same dtype (got %d and %d)", A->value_dtype, dtype);
   if (!valid_bs(bs)) return set_error(h, TRL_ENOTSUP, "unsupported block size %d", bs);
   if (A->n < 0 || A->nnz < 0 || A->nnz >= (int64_t(1) << 31)) return set_error(h, TRL_EINVAL, "bad CSR sizes");
   if (A->n == 0) return TRL_OK;
   if (!A->rowptr || (A->nnz > 0 && (!A->colind || !A->values))) return set_error(h, TRL_EINVAL, "null CSR array");
-  if (X == Y || (W && W == X)) return set_error(h, TRL_EINVAL, "SpMM input must alias neither output nor third operand");
   const size_t es = dtype == TRL_F64 ? 8 : 4;
+  const auto overlap = [&](const void* a, const void* b) {
+    const auto pa = reinterpret_cast<uintptr_t>(a), pb = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t len = static_cast<uintptr_t>(nb) * A->n * bs * es;
+    return pa < pb + len && pb < pa + len;
+  };
+  if (overlap(X, Y) || (W && overlap(W, X)) || (W && W != Y && overlap(W, Y)))
+    return set_error(h, TRL_EINVAL, "SpMM input must overlap neither output nor third operand");
   if (((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) % (es * bs < 16 ? es * bs : 16)) != 0)
     return set_error(h, TRL_EINVAL, "block vectors must be aligned to min(16, bs*elem) bytes");
-  ProfScope prof(h, PROF_SPMM, A->nnz * (es + 4.0) + 4.0 * (A->n + 1) + (W ? 3.0 : 2.0) * A->n * bs * es, 2.0 * A->nnz * bs);
+  ProfScope prof(h, PROF_SPMM, A->nnz * (es + 4.0) + 4.0 * (A->n + 1) + nb * (W ? 3.0 : 2.0) * A->n * bs * es, 2.0 * A->nnz * bs * nb);
   int st = TRL_OK;
   TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
     using S = SpmmShape<T, BS>;
     // one resident wave: every warp strides over the rows (its rowptr prefetch pays off)
-    static int resident = 0;
-    if (resident == 0) {
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_spmm<T, BS>, kThreads, 0) != cudaSuccess || resident < 1) resident = S::MINB;
-      cudaGetLastError();
-    }
-    const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, resident);
-    k_spmm<T, BS><<<grid, kThreads, 0, h->stream>>>(A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
-                                                    static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma), static_cast<const T*>(W));
+    const auto launch = [&](auto kernel) {
+      static int resident = 0; // one per instantiation of the kernel
+      if (resident == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads, 0) != cudaSuccess || resident < 1) resident = S::MINB;
+        cudaGetLastError();
+      }
+      const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, resident);
+      kernel<<<grid, kThreads, 0, h->stream>>>(A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
+                                               static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma), static_cast<const T*>(W), nb, A->n * BS);
+    };
+    if (nb > 1) launch(k_spmm<T, BS, true>);
+    else launch(k_spmm<T, BS, false>);
     st = after_launch(h, "spmm");
   }));
   return st;
@@ -265,13 +291,19 @@ static int spmm_impl(trl_cuda_context* h, const trl_csr* A, int dtype, const voi
 int trl_cuda_spmm(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta)
 {
   TRL_CHECK_HANDLE(h);
-  return spmm_impl(h, A, dtype, X, Y, bs, alpha, beta, 0.0, nullptr);
+  return spmm_impl(h, A, dtype, X, Y, bs, 1, alpha, beta, 0.0, nullptr);
 }
 
 int trl_cuda_spmm3(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, double alpha, double beta, double gamma, const void* W)
 {
   TRL_CHECK_HANDLE(h);
-  return spmm_impl(h, A, dtype, X, Y, bs, alpha, beta, gamma, W);
+  return spmm_impl(h, A, dtype, X, Y, bs, 1, alpha, beta, gamma, W);
+}
+
+int trl_cuda_spmm_blocks(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, int nb, double alpha, double beta, double gamma, const void* W)
+{
+  TRL_CHECK_HANDLE(h);
+  return spmm_impl(h, A, dtype, X, Y, bs, nb, alpha, beta, gamma, W);
 }
 
 int trl_cuda_sddmm(trl_cuda_handle h, const trl_csr* P, const double* X, int k, const double* w, double* out)

@@ -59,6 +59,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_spmm": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double]),
     "trl_cuda_csr_norm1": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "trl_cuda_spmm3": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double, C.c_double, P]),
+    "trl_cuda_spmm_blocks": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, P]),
     "trl_cuda_csr_gershgorin": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "trl_cuda_sddmm": (C.c_int, [P, P, P, C.c_int, P, P]),
     "trl_cuda_eigen_adjoint": (C.c_int, [P, P, P, C.c_int, P, P, C.c_double, C.c_int, P]),
@@ -250,6 +251,10 @@ class Handle:
     def spmm3(self, A: "DeviceCSRTensors", X, Y, alpha: float, beta: float, gamma: float, W):
         n, bs = X.shape
         self.check(self.lib.trl_cuda_spmm3(self.h, C.byref(A.desc), _dtype(X), _ptr(X), _ptr(Y), bs, alpha, beta, gamma, _ptr(W)))
+
+    def spmm_blocks(self, A: "DeviceCSRTensors", X, Y, alpha: float, beta: float, gamma: float, W):
+        nb, n, bs = X.shape
+        self.check(self.lib.trl_cuda_spmm_blocks(self.h, C.byref(A.desc), _dtype(X), _ptr(X), _ptr(Y), bs, nb, alpha, beta, gamma, _ptr(W)))
 
     def csr_gershgorin(self, A: "DeviceCSRTensors", alpha: float = 1.0, beta: float = 0.0):
         lo, hi = C.c_double(0.0), C.c_double(0.0)
