@@ -276,9 +276,11 @@ def trl_arm(args, world, rank, local):
                        "l2": "inputs larger than L2 (basis 2.8 GB, CSR 113 MB, per-step working set >> 126 MB)"},
             "fp64": {"seconds": ms64 / 1e3, "restarts": o64["restarts"], "n_op_apply": o64["n_op_apply"], "converged": bool(o64["converged"]),
                      "max_rel_residual": o64["max_rel_residual"], "max_rel_err_vs_analytic": err64},
-            "mixed": {"seconds": msmx / 1e3, "speedup_vs_fp64": ms64 / msmx, "refine": "chebyshev-filtered subspace iteration + Rayleigh-Ritz (FP64)",
+            "mixed": {"seconds": msmx / 1e3, "speedup_vs_fp64": ms64 / msmx,
+                      "refine": "Chebyshev-filtered subspace iteration + Rayleigh-Ritz on nev/bs+2 blocks (FP32 filter rounds, then FP64)",
                       "restarts_fp32": omx["restarts_fp32"], "n_op_apply_fp32": omx["n_op_apply_fp32"], "seconds_fp32_phase": omx["seconds_fp32"],
-                      "refine_rounds": omx["refine_rounds"], "refine_degree": omx["refine_degree"], "fp32_tol": args.fp32_tol,
+                      "refine_rounds": omx["refine_rounds"], "refine_degree": omx["refine_degree"],
+                      "refine_degree_fp32": omx["refine_degree_fp32"], "fp32_tol": args.fp32_tol,
                       "converged": bool(omx["converged"]), "max_rel_residual": omx["max_rel_residual"], "max_theta_residual": omx["max_theta_residual"],
                       "max_rel_err_vs_analytic": errmx},
             "mixed_lanczos_refine": {"seconds": mslz / 1e3, "speedup_vs_fp64": ms64 / mslz, "restarts_fp32": olz["restarts_fp32"],
@@ -410,7 +412,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
-    ap.add_argument("--fp32-tol", type=float, default=1e-4)
+    ap.add_argument("--fp32-tol", type=float, default=3e-3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", choices=["solve", "spmm", "dot", "update", "project", "rotate"], default=None,
                     help="profiling driver: run one piece of the workload and exit (see profile_case)")

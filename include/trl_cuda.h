@@ -95,7 +95,13 @@ int trl_cuda_profile_enable(trl_cuda_handle handle, int on);
 /* Synchronises the stream and copies the TRL_PROF_CLASSES totals into out. */
 int trl_cuda_profile_read(trl_cuda_handle handle, trl_kernel_stats* out);
 
-/* ---- memory (replaces aligned host allocation: multivector.hh:44-48, blockmatrix.hh:28-32) */
+/* ---- memory (replaces aligned host allocation: multivector.hh:44-48, blockmatrix.hh:28-32)
+ * Device memory from the handle's memory pool (256-byte aligned, usable from any stream on
+ * return). The pool keeps freed memory reserved until the handle is destroyed, so repeated
+ * solves reuse it instead of returning it to the driver. trl_cuda_free takes a block from
+ * trl_cuda_malloc of the same handle and returns it to the pool in the order of the handle's
+ * stream: work queued there before the call may still use it; work on other streams that
+ * uses it must have finished. */
 int trl_cuda_malloc(trl_cuda_handle handle, void** ptr, size_t bytes);
 int trl_cuda_free(trl_cuda_handle handle, void* ptr);
 /* Asynchronous copy on the handle's stream; TRL_D2H waits for completion before returning. */

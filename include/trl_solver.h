@@ -55,6 +55,9 @@ typedef struct trl_solve_params {
   int batching;                  /* fuse the restart rotation (see trl::cuda::Context) */
   unsigned seed;                 /* seed of the refinement's random combination */
   int refine;                    /* trl_refine (TRL_MODE_MIXED) */
+  unsigned fp32_ncv;             /* TRL_MODE_MIXED: basis size of the FP32 phase (0: ncv) */
+  int refine_fp32;               /* TRL_REFINE_CHEBYSHEV: filter in FP32 while the residual is
+                                    above ~2e-5, then in FP64 (0: FP64 only) */
 } trl_solve_params;
 
 typedef struct trl_solve_info {
@@ -73,13 +76,17 @@ typedef struct trl_solve_info {
   double h2d_bytes, d2h_bytes;        /* host<->device traffic of the call */
   unsigned refine_rounds;   /* TRL_REFINE_CHEBYSHEV: Rayleigh-Ritz rounds (0: not used) */
   unsigned refine_degree;   /* TRL_REFINE_CHEBYSHEV: total filter degree */
+  unsigned refine_degree_fp32; /* TRL_REFINE_CHEBYSHEV: of which applied in FP32 */
 } trl_solve_info;
 
 void trl_solve_params_default(trl_solve_params* p);
 
 /* Host in, host out: uploads the CSR operator and X0 (n x bs row-major), solves, and
  * returns evals[nev], optionally evecs (n x nev row-major) and resid[nev]
- * (||op x - theta x|| / ||op||_1). Creates and destroys its own handle on `device`. */
+ * (||op x - theta x|| / ||op||_1). Runs on a handle of its own on `device`, created by the
+ * first call and kept until the process exits together with the device memory its pool
+ * holds (the peak of the calls so far), so that later calls reuse it; calls on one device
+ * are serialised. */
 int trl_solve_csr_host(const trl_solve_params* p, int device, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind, const double* values, const double* X0,
                        double* evals, double* evecs, double* resid, trl_solve_info* info);
 

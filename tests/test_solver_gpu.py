@@ -113,12 +113,14 @@ def test_cfg1_mixed_reaches_fp64_accuracy(cfg1_oracle):
     assert out["restarts_fp32"] > 0
 
 
-@pytest.mark.parametrize("refine", [native.TRL_REFINE_CHEBYSHEV, native.TRL_REFINE_LANCZOS])
-def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine):
+@pytest.mark.parametrize("refine,refine_fp32", [(native.TRL_REFINE_CHEBYSHEV, 1), (native.TRL_REFINE_CHEBYSHEV, 0), (native.TRL_REFINE_LANCZOS, 1)])
+def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine, refine_fp32):
     """Both FP64 refinements of the mixed mode from the FP32 phase's kept Ritz vectors: the
-    Chebyshev-filtered subspace iteration with Rayleigh-Ritz, and a BlockLanczos restart."""
+    Chebyshev-filtered subspace iteration with Rayleigh-Ritz (with and without its FP32
+    filter rounds), and a BlockLanczos restart."""
     A, X0, ref = cfg1_oracle
-    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4, refine=refine)
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4, refine=refine,
+                                refine_fp32=refine_fp32)
     assert out["converged"]
     exact = P.laplace2d_eigenvalues(128)[:10]
     assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-11
@@ -127,8 +129,30 @@ def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine):
     assert max_principal_sine(out["evecs"], ref["ritz"], out["evals"]) < 1e-5
     if refine == native.TRL_REFINE_CHEBYSHEV:
         assert out["refine_rounds"] >= 1 and out["refine_degree"] > 0 and out["restarts"] == 0
+        if not refine_fp32:
+            assert out["refine_degree_fp32"] == 0
     else:
         assert out["refine_rounds"] == 0 and out["restarts"] > 0
+
+
+@pytest.mark.parametrize("fp32_ncv", [0, 96])
+def test_mixed_loose_fp32_phase_filters_in_fp32(cfg1_oracle, fp32_ncv):
+    """A loose FP32 phase (fp32_tol 1e-2, optionally on a smaller FP32 basis) leaves most of
+    the work to the filter: its FP32 rounds run first and the FP64 rounds finish at 1e-10."""
+    A, X0, ref = cfg1_oracle
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-2, fp32_ncv=fp32_ncv)
+    assert out["converged"]
+    assert 0 < out["refine_degree_fp32"] < out["refine_degree"]
+    exact = P.laplace2d_eigenvalues(128)[:10]
+    assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-11
+    assert out["max_theta_residual"] < 1e-10
+    assert max_principal_sine(out["evecs"], ref["ritz"], out["evals"]) < 1e-5
+
+
+def test_fp32_ncv_must_be_a_multiple_of_the_block_size(cfg1_oracle):
+    A, X0, _ = cfg1_oracle
+    with pytest.raises(native.TrlError):
+        native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_ncv=98)
 
 
 def test_mixed_with_kept_values_on_both_sides_of_zero_uses_lanczos(oracle):

@@ -19,6 +19,7 @@ struct trl_cuda_context {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr; // trl_cuda_malloc's stream-ordered pool (created on first use)
   bool owns_stream = false;
   int* d_status = nullptr;  // device status word
   void* ws = nullptr;       // growable device workspace (per-call partial sums)

@@ -17,9 +17,13 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -130,36 +134,43 @@ PhaseOut run_phase_r(const std::shared_ptr<Context>& ctx, const trl_csr* A, cons
 
 // ---- FP64 refinement of the mixed mode by Chebyshev-filtered subspace iteration ---------
 //
-// The FP32 phase leaves kr = nev/bs + 1 blocks of Ritz vectors accurate to about fp32_tol.
-// Their span already holds the wanted eigenvectors up to that accuracy; what is left is to
-// damp the components along the rest of the spectrum. A Chebyshev polynomial of degree d on
-// the interval [a, b] that holds every unwanted eigenvalue (a a Gershgorin bound, b the
-// smallest kept Ritz value) amplifies an eigenvector with eigenvalue x > b by
-// T_d((x - c) / e) (c, e the interval's centre and half-width) relative to the damped ones.
-// The filter is applied with the three-term recurrence in the scaled form of Zhou & Saad
-// (2007, "Chebyshev-filtered subspace iteration"), one multi-block SpMM per degree that
-// reads the CSR stream once for all kept blocks; the block is re-orthonormalised whenever
-// the spread of amplifications across the kept vectors reaches about 1e6, and a
-// Rayleigh-Ritz step (dense kr*bs eigenproblem) follows every filter round. The Ritz pairs are final when every wanted pair has
-// ||op x - theta x|| / |theta| < tol (the driver's convergence test, evp_base.hh:128-147).
-// No Krylov basis is built, so there is no reorthogonalisation against a growing basis:
-// each degree costs one CSR pass plus the kr blocks' gathers and stores.
+// The FP32 phase hands over nev/bs + 2 blocks of Ritz vectors (one block more than the
+// thick restart keeps) accurate to about fp32_tol. Their span already holds the wanted
+// eigenvectors up to that accuracy; what is left is to damp the components along the rest
+// of the spectrum. A Chebyshev polynomial of degree d on the interval [a, b] that holds
+// every unwanted eigenvalue (a a Gershgorin bound, b the smallest kept Ritz value)
+// amplifies an eigenvector with eigenvalue x > b by T_d((x - c) / e) (c, e the interval's
+// centre and half-width) relative to the damped ones. The filter is applied with the
+// three-term recurrence in the scaled form of Zhou & Saad (2007, "Chebyshev-filtered
+// subspace iteration"), one multi-block SpMM per degree that reads the CSR stream once for
+// all kept blocks. The block is re-orthonormalised whenever the spread of amplifications
+// across the kept vectors reaches about 1e6 (1e3 in FP32), and a Rayleigh-Ritz step (dense
+// eigenproblem of the kept vectors, FP64) follows every filter round; a round aims at two
+// orders of magnitude at most. Rounds filter in FP32 (FP32 operator and vectors, half the
+// bytes per degree) while the wanted residual is above what FP32 vectors resolve, then in
+// FP64. The Ritz pairs are final when every wanted pair has ||op x - theta x|| / |theta| <
+// tol (the driver's convergence test, evp_base.hh:128-147). No Krylov basis is built, so
+// there is no reorthogonalisation against a growing basis: each degree costs one CSR pass
+// plus the kept blocks' gathers and stores.
 
 struct RefineOut {
   bool applicable = false; // false: the kept Ritz values straddle zero (use the Lanczos refinement)
   bool converged = false;
   unsigned rounds = 0;
-  unsigned degree = 0;
+  unsigned degree = 0;   // total filter degree (FP32 and FP64 rounds)
+  unsigned degree32 = 0; // of which FP32
   std::vector<double> evals; // Ritz values of the last Rayleigh-Ritz step, |theta| descending
 };
 
 template <unsigned bs>
 class ChebyshevRefinement {
 public:
-  ChebyshevRefinement(std::shared_ptr<Context> ctx, const trl_csr* A, const trl_solve_params& p, unsigned kr)
+  /// A32 (may be null): the FP32 copy of the operator, for the FP32 filter rounds.
+  ChebyshevRefinement(std::shared_ptr<Context> ctx, const trl_csr* A, const trl_csr* A32, const trl_solve_params& p, unsigned kr)
       : ctx_(std::move(ctx))
       , h_(ctx_->handle())
       , A_(A)
+      , A32_(A32)
       , p_(p)
       , kr_(kr)
       , n_(A->n)
@@ -173,6 +184,8 @@ public:
       , Z_(ctx_, sizeof(double) * kr * kr * bs * bs)
       , ev_(ctx_, sizeof(double) * kr * bs)
       , small_(ctx_, sizeof(double) * 4 * bs * bs)
+      , X32_(ctx_, A32 ? sizeof(float) * blk_ * kr : 0)
+      , Y32_(ctx_, A32 ? sizeof(float) * blk_ * kr : 0)
   {
   }
 
@@ -187,6 +200,8 @@ public:
     double* spare = static_cast<double*>(Y_.get());
     orthonormalize(cur);
     const unsigned N = kr_ * bs;
+    bool use32 = A32_ != nullptr;
+    double prev_res = 0.0; // residual at the start of the last FP32 round
     for (unsigned round = 0; round < kMaxRounds; ++round) {
       std::vector<double> theta = rayleigh_ritz(cur, spare); // cur <- Ritz vectors (in spare, swapped)
       std::swap(cur, spare);
@@ -215,20 +230,54 @@ public:
       if (!(e > 0.0) || !(worst > b)) return finish(out, cur, X);
       const double xw = (worst - c) / e, xt = (top - c) / e;
       const double rw = std::acosh(xw), rt = std::acosh(std::max(xt, xw));
-      // degree: reduce the worst wanted residual to a tenth of the tolerance
-      const double need = std::log(2.0 * std::max(res / (0.1 * p_.tol), 2.0));
-      unsigned d = static_cast<unsigned>(std::ceil(need / rw));
+      // FP32 rounds while the residual is above what FP32 vectors resolve and FP32 rounds
+      // still make progress (a round that gains less than 1.05x has met the FP32 floor)
+      if (use32 && prev_res > 0.0 && !(res < prev_res / 1.05)) use32 = false;
+      if (use32 && !(res > kFp32Floor)) use32 = false;
+      prev_res = use32 ? res : 0.0;
+      // degree: reduce the worst wanted residual to a tenth of the tolerance (FP32 rounds:
+      // to the FP32 target), at most two orders of magnitude per round. The predicted rate
+      // acosh((worst - c) / e) assumes accurate Ritz values; early on the smallest kept one
+      // (b) is too low and the rate several times too high, so a round undershoots and the
+      // next Rayleigh-Ritz step (a few ms) re-estimates, instead of one long round
+      // overshooting. A round runs kMinDegree degrees at least unless fewer finish the job,
+      // so that early rounds are not dominated by their Rayleigh-Ritz step.
+      const double target = use32 ? std::max(0.1 * p_.tol, kFp32Target) : 0.1 * p_.tol;
+      const double need_all = std::log(2.0 * std::max(res / target, 2.0));
+      const double need = std::min(need_all, std::log(100.0));
+      const unsigned d_all = static_cast<unsigned>(std::ceil(need_all / rw));
+      unsigned d = std::max(static_cast<unsigned>(std::ceil(need / rw)), std::min(kMinDegree, d_all));
       d = std::clamp(d, 8u, kMaxDegree);
       // chunk length: re-orthonormalise before the spread of amplifications exceeds ~1e6
+      // (~1e3 in FP32, whose rounding would otherwise swamp the least amplified vectors)
       const double spread = rt - rw;
-      unsigned chunk = spread > 0.0 ? static_cast<unsigned>(std::log(1e6) / spread) : d;
+      unsigned chunk = spread > 0.0 ? static_cast<unsigned>(std::log(use32 ? 1e3 : 1e6) / spread) : d;
       chunk = std::clamp(chunk, 4u, d);
       unsigned done = 0;
-      while (done < d) {
-        const unsigned L = std::min(chunk, d - done);
-        if (filter(cur, spare, L, s, c, e, top) == spare) std::swap(cur, spare); // the filtered block is in cur
+      if (trace_)
+        std::fprintf(stderr, "refine round %u fp32 %d res %.3e degree %u rate %.4f chunk %u b %.6f worst %.6f host %.1f ms\n", round, static_cast<int>(use32), res, d, rw, chunk, b,
+                     worst, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count());
+      if (use32) {
+        float* c32 = static_cast<float*>(X32_.get());
+        float* s32 = static_cast<float*>(Y32_.get());
+        ctx_->check(trl_cuda_convert(h_, TRL_F32, c32, TRL_F64, cur, static_cast<std::int64_t>(blk_) * kr_), "refine narrow");
+        while (done < d) {
+          const unsigned L = std::min(chunk, d - done);
+          if (filter(A32_, c32, s32, L, s, c, e, top) == s32) std::swap(c32, s32);
+          orthonormalize(c32);
+          done += L;
+        }
+        ctx_->check(trl_cuda_convert(h_, TRL_F64, cur, TRL_F32, c32, static_cast<std::int64_t>(blk_) * kr_), "refine widen");
         orthonormalize(cur);
-        done += L;
+        out.degree32 += d;
+      }
+      else {
+        while (done < d) {
+          const unsigned L = std::min(chunk, d - done);
+          if (filter(A_, cur, spare, L, s, c, e, top) == spare) std::swap(cur, spare); // the filtered block is in cur
+          orthonormalize(cur);
+          done += L;
+        }
       }
       out.degree += d;
     }
@@ -237,19 +286,32 @@ public:
   }
 
 private:
-  static constexpr unsigned kMaxRounds = 12;
+  static constexpr unsigned kMaxRounds = 40;
   static constexpr unsigned kMaxDegree = 4000;
+  static constexpr unsigned kMinDegree = 64;
+  // FP32 filter rounds run while the wanted residual is above kFp32Floor and aim at
+  // kFp32Target: FP32 vectors resolve ||op x - theta x|| / |theta| to about 4e-6 on the
+  // 96^3 workload
+  static constexpr double kFp32Floor = 2e-5;
+  static constexpr double kFp32Target = 3e-6;
 
   std::shared_ptr<Context> ctx_;
   trl_cuda_handle h_;
   const trl_csr* A_;
+  const trl_csr* A32_;
   trl_solve_params p_;
   unsigned kr_;
   std::int64_t n_;
   std::size_t blk_;
-  DeviceBuffer Y_, AX_, AXr_, R_, T_, C_, Z_, ev_, small_;
+  DeviceBuffer Y_, AX_, AXr_, R_, T_, C_, Z_, ev_, small_, X32_, Y32_;
+  const bool trace_ = std::getenv("TRL_REFINE_TRACE") != nullptr; // per-round log on stderr
+  const std::chrono::steady_clock::time_point t0_ = std::chrono::steady_clock::now();
 
-  double* blockp(double* base, unsigned j) const { return base + static_cast<std::size_t>(j) * blk_; }
+  template <class T>
+  T* blockp(T* base, unsigned j) const
+  {
+    return base + static_cast<std::size_t>(j) * blk_;
+  }
 
   /// Leaves the current block in the caller's buffer.
   RefineOut& finish(RefineOut& out, double* cur, double* X)
@@ -259,13 +321,15 @@ private:
   }
 
   /// Block classical Gram-Schmidt (two passes) across the kr blocks, then CholQR2 per block.
-  void orthonormalize(double* X)
+  template <class T>
+  void orthonormalize(T* X)
   {
+    constexpr int dt = trl::cuda::dtype_of<T>::value;
     double* G = static_cast<double*>(small_.get());
     double* R = G + bs * bs;
     for (unsigned j = 0; j < kr_; ++j) {
-      if (j > 0) ctx_->check(trl_cuda_project_out(h_, TRL_F64, X, static_cast<int>(j), blockp(X, j), n_, bs, TRL_CGS_TWO, 0.0, G), "refine orthonormalize");
-      ctx_->check(trl_cuda_cholqr_gram(h_, TRL_F64, blockp(X, j), n_, bs, 2, R, j > 0 ? G : nullptr), "refine orthonormalize");
+      if (j > 0) ctx_->check(trl_cuda_project_out(h_, dt, X, static_cast<int>(j), blockp(X, j), n_, bs, TRL_CGS_TWO, 0.0, G), "refine orthonormalize");
+      ctx_->check(trl_cuda_cholqr_gram(h_, dt, blockp(X, j), n_, bs, 2, R, j > 0 ? G : nullptr), "refine orthonormalize");
     }
   }
 
@@ -325,20 +389,22 @@ private:
   /// p_L(s op) X with the scaled Chebyshev recurrence on [c - e, c + e], normalised at the
   /// point `top` (the largest kept value) so that the kept components stay O(1). X and Y are
   /// the two recurrence buffers (both overwritten); returns the one holding the result.
-  double* filter(double* X, double* Y, unsigned L, double s, double c, double e, double top)
+  template <class T>
+  T* filter(const trl_csr* A, T* X, T* Y, unsigned L, double s, double c, double e, double top)
   {
+    constexpr int dt = trl::cuda::dtype_of<T>::value;
     // s * op = s*alpha*A + s*beta*I; the recurrence needs (s*op - c) / e
     const double al = s * p_.alpha, be = s * p_.beta - c;
     double sigma = e / (top - c);
     const double tau = 2.0 / sigma;
     // Y1 = (s op - c) X * sigma / e
-    ctx_->check(trl_cuda_spmm_blocks(h_, A_, TRL_F64, X, Y, bs, static_cast<int>(kr_), al * sigma / e, be * sigma / e, 0.0, nullptr), "refine filter");
-    double* prev = X;
-    double* curv = Y;
+    ctx_->check(trl_cuda_spmm_blocks(h_, A, dt, X, Y, bs, static_cast<int>(kr_), al * sigma / e, be * sigma / e, 0.0, nullptr), "refine filter");
+    T* prev = X;
+    T* curv = Y;
     for (unsigned i = 2; i <= L; ++i) {
       const double sigma2 = 1.0 / (tau - sigma);
       // Y_{i} = 2 sigma2 / e (s op - c) Y_{i-1} - sigma sigma2 Y_{i-2}, written over Y_{i-2}
-      ctx_->check(trl_cuda_spmm_blocks(h_, A_, TRL_F64, curv, prev, bs, static_cast<int>(kr_), 2.0 * sigma2 / e * al, 2.0 * sigma2 / e * be, -sigma * sigma2, prev),
+      ctx_->check(trl_cuda_spmm_blocks(h_, A, dt, curv, prev, bs, static_cast<int>(kr_), 2.0 * sigma2 / e * al, 2.0 * sigma2 / e * be, -sigma * sigma2, prev),
                   "refine filter");
       std::swap(prev, curv);
       sigma = sigma2;
@@ -355,12 +421,22 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
   const std::int64_t n = A64->n;
   const unsigned kx = (p.nev + bs - 1) / bs; // blocks of Ritz vectors to form
   const unsigned kr = p.nev / bs + 1;        // blocks the thick restart keeps (lanczos.hh:97)
+  // blocks the Chebyshev refinement iterates on: one more than the restart keeps. Its cost
+  // per order of magnitude is ~ blocks / acosh(1 + 2 (theta_nev - theta_last) / (theta_last -
+  // a)); on the 96^3 workload (nev 32, bs 8) that is 306 for 5 blocks, 231 for 6, ~228 for 7-8.
+  const unsigned kref = kr + 1;
   cudaStream_t stream = static_cast<cudaStream_t>(trl_cuda_stream(h));
   const auto launches0 = trl_cuda_launch_count(h);
 
   EventTimer total(stream), phase(stream);
   total.start();
-  DeviceBuffer X64(ctx, sizeof(double) * static_cast<std::size_t>(n) * bs * std::max(kx, kr));
+  // TRL_REFINE_TRACE: host timestamps of the solve's stages on stderr
+  const bool trace = std::getenv("TRL_REFINE_TRACE") != nullptr;
+  const auto host0 = std::chrono::steady_clock::now();
+  const auto stage = [&](const char* what) {
+    if (trace) std::fprintf(stderr, "solve %s host %.1f ms\n", what, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count());
+  };
+  DeviceBuffer X64(ctx, sizeof(double) * static_cast<std::size_t>(n) * bs * std::max(kx, kref));
   PhaseOut out;
   double t32 = 0.0;
 
@@ -369,7 +445,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
   }
   else {
     if (!A32) throw std::invalid_argument("FP32 and mixed modes need the FP32 copy of the operator");
-    DeviceBuffer X32(ctx, sizeof(float) * static_cast<std::size_t>(n) * bs * std::max(kx, kr));
+    DeviceBuffer X32(ctx, sizeof(float) * static_cast<std::size_t>(n) * bs * std::max(kx, kref));
     DeviceBuffer X0f(ctx, sizeof(float) * static_cast<std::size_t>(n) * bs);
     ctx->check(trl_cuda_convert(h, TRL_F32, X0f.get(), TRL_F64, X0, n * bs), "initial block");
     if (p.mode == TRL_MODE_FP32) {
@@ -378,18 +454,24 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
     }
     else {
       phase.start();
-      PhaseOut o32 = run_phase_r<float, bs>(ctx, A32, p, p.max_restarts, p.fp32_tol, static_cast<const float*>(X0f.get()), kr, static_cast<float*>(X32.get()));
+      trl_solve_params p32 = p;
+      if (p.fp32_ncv) p32.ncv = p.fp32_ncv;
+      const unsigned k32 = std::min(kref, p32.ncv / bs); // Ritz blocks the FP32 phase hands over
+      PhaseOut o32 = run_phase_r<float, bs>(ctx, A32, p32, p.max_restarts, p.fp32_tol, static_cast<const float*>(X0f.get()), k32, static_cast<float*>(X32.get()));
       t32 = phase.stop();
+      stage("fp32 phase done");
       info->restarts_fp32 = o32.restarts;
       info->n_op_apply_fp32 = o32.applies;
       // FP64 refinement: widen the kept FP32 Ritz vectors and start the FP64 solve from a
       // seeded random combination of them (the start block then carries every wanted
       // direction to FP32 accuracy).
-      ctx->check(trl_cuda_convert(h, TRL_F64, X64.get(), TRL_F32, X32.get(), n * bs * kr), "widen");
+      ctx->check(trl_cuda_convert(h, TRL_F64, X64.get(), TRL_F32, X32.get(), n * bs * k32), "widen");
       bool refined = false;
       if (p.refine == TRL_REFINE_CHEBYSHEV) {
-        ChebyshevRefinement<bs> cheb(ctx, A64, p, kr);
+        ChebyshevRefinement<bs> cheb(ctx, A64, p.refine_fp32 ? A32 : nullptr, p, k32);
+        stage("refinement buffers allocated");
         const RefineOut r = cheb.run(static_cast<double*>(X64.get()));
+        stage("refinement done");
         if (r.applicable) {
           refined = true;
           out.converged = r.converged;
@@ -398,6 +480,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
           out.evals = r.evals;
           info->refine_rounds = r.rounds;
           info->refine_degree = r.degree;
+          info->refine_degree_fp32 = r.degree32;
         }
       }
       if (!refined) {
@@ -421,6 +504,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
   info->seconds_fp32 = t32;
   for (unsigned c = 0; c < p.nev; ++c) evals_host[c] = c < out.evals.size() ? out.evals[c] : 0.0;
 
+  stage("eigenpairs found");
   // ---- Ritz vectors and true residuals, FP64 ----
   info->max_rel_residual = info->max_theta_residual = 0.0;
   if (p.want_vectors) {
@@ -459,6 +543,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
     info->seconds_vectors = phase.stop();
   }
   info->seconds = total.stop();
+  stage("residuals done");
   info->kernel_launches = trl_cuda_launch_count(h) - launches0;
   return TRL_OK;
 }
@@ -482,11 +567,31 @@ int fail(const std::exception& e, int status)
   return status;
 }
 
+// trl_solve_csr_host's context on each device: created by the first call and kept until
+// the process exits, so that its memory pool keeps the solve's buffers reserved between
+// calls (allocating and freeing a solve's 4-6 GB each call cost up to a second of host time
+// on B200). Calls on one device are serialised.
+struct HostContext {
+  std::mutex m;
+  std::shared_ptr<Context> ctx;
+};
+
+HostContext& host_context(int device)
+{
+  static std::mutex registry_lock;
+  static auto* registry = new std::map<int, std::unique_ptr<HostContext>>(); // never destroyed: outlives static teardown
+  std::lock_guard<std::mutex> g(registry_lock);
+  auto& slot = (*registry)[device];
+  if (!slot) slot = std::make_unique<HostContext>();
+  return *slot;
+}
+
 void validate(const trl_solve_params* p)
 {
   if (!p) throw std::invalid_argument("null params");
   if (p->mode < TRL_MODE_FP64 || p->mode > TRL_MODE_MIXED) throw std::invalid_argument("bad mode");
   if (p->ncv % p->bs != 0) throw std::invalid_argument("ncv must be a multiple of the block size");
+  if (p->fp32_ncv % p->bs != 0) throw std::invalid_argument("fp32_ncv must be a multiple of the block size");
   if (p->cholqr_passes < 1 || p->cholqr_passes > 4) throw std::invalid_argument("cholqr_passes must be in [1, 4]");
   if (p->reorth < TRL_REORTH_MGS || p->reorth > TRL_REORTH_CGS1) throw std::invalid_argument("bad reorth strategy");
   if (p->refine != TRL_REFINE_LANCZOS && p->refine != TRL_REFINE_CHEBYSHEV) throw std::invalid_argument("bad refinement");
@@ -510,12 +615,13 @@ void trl_solve_params_default(trl_solve_params* p)
   p->beta = 0.0;
   p->reorth = TRL_REORTH_CGS_IFNEEDED;
   p->cholqr_passes = 2;
-  p->fp32_tol = 1e-4; // 96^3 workload, Chebyshev refinement: 18 FP32 restarts + filter degree 1243 (0.87 s; 1e-2: 0.76 s, 1e-5: 0.98 s)
+  p->fp32_tol = 3e-3; // 96^3 workload: 4 FP32 restarts, then filter degree ~1170 of which ~640 in FP32 (0.42 s; 1e-2 and 3e-2 within noise, 1e-3: 0.53 s)
   p->refine_max_restarts = 1000;
   p->want_vectors = 1;
   p->batching = 1;
   p->seed = 42;
   p->refine = TRL_REFINE_CHEBYSHEV;
+  p->refine_fp32 = 1;
 }
 
 const char* trl_solver_last_error(void) { return g_err.c_str(); }
@@ -544,11 +650,16 @@ int trl_solve_csr_device(trl_cuda_handle h, const trl_solve_params* p, const trl
 int trl_solve_csr_host(const trl_solve_params* p, int device, int64_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colind, const double* values, const double* X0,
                        double* evals, double* evecs, double* resid, trl_solve_info* info)
 {
+  HostContext* hc = nullptr;
+  std::unique_lock<std::mutex> lock;
   try {
     validate(p);
     if (!rowptr || !X0 || !evals || !info || (nnz > 0 && (!colind || !values))) throw std::invalid_argument("null argument");
     *info = trl_solve_info{};
-    auto ctx = Context::create(device, nullptr);
+    hc = &host_context(device);
+    lock = std::unique_lock<std::mutex>(hc->m);
+    if (!hc->ctx) hc->ctx = Context::create(device, nullptr);
+    auto ctx = hc->ctx;
     ctx->set_batching(p->batching != 0);
     const auto h = ctx->handle();
     double h2d = 0.0, d2h = 0.0;
@@ -579,9 +690,11 @@ int trl_solve_csr_host(const trl_solve_params* p, int device, int64_t n, int64_t
     return TRL_OK;
   }
   catch (const std::invalid_argument& e) {
+    if (hc && lock.owns_lock()) hc->ctx.reset(); // a failed call may leave recorded work behind: start afresh
     return fail(e, TRL_EINVAL);
   }
   catch (const std::exception& e) {
+    if (hc && lock.owns_lock()) hc->ctx.reset();
     const std::string w = e.what();
     return fail(e, w.find("Cholesky") != std::string::npos ? TRL_ECHOLESKY : (w.find("Eigendecomposition") != std::string::npos ? TRL_EEIGEN : TRL_ECUDA));
   }

@@ -87,7 +87,8 @@ class trl_solve_params(C.Structure):
     _fields_ = [("bs", C.c_int), ("mode", C.c_int), ("nev", C.c_uint), ("ncv", C.c_uint), ("max_restarts", C.c_uint),
                 ("tol", C.c_double), ("alpha", C.c_double), ("beta", C.c_double), ("reorth", C.c_int),
                 ("cholqr_passes", C.c_int), ("fp32_tol", C.c_double), ("refine_max_restarts", C.c_uint),
-                ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint), ("refine", C.c_int)]
+                ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint), ("refine", C.c_int),
+                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int)]
 
 
 class trl_solve_info(C.Structure):
@@ -95,7 +96,8 @@ class trl_solve_info(C.Structure):
                 ("n_op_apply_fp32", C.c_uint), ("seconds", C.c_double), ("seconds_fp32", C.c_double),
                 ("seconds_vectors", C.c_double), ("max_rel_residual", C.c_double), ("max_theta_residual", C.c_double),
                 ("op_norm1", C.c_double), ("kernel_launches", C.c_ulonglong), ("h2d_bytes", C.c_double), ("d2h_bytes", C.c_double),
-                ("refine_rounds", C.c_uint), ("refine_degree", C.c_uint)]
+                ("refine_rounds", C.c_uint), ("refine_degree", C.c_uint),
+                ("refine_degree_fp32", C.c_uint)]
 
 
 SOLVER_SYMBOLS = {
