@@ -15,6 +15,7 @@
 #include "multivector.hh"
 
 #include <cassert>
+#include <algorithm>
 #include <cstddef>
 #include <memory>
 #include <optional>
@@ -84,9 +85,18 @@ public:
                    {evals_dev_.get(), sizeof(double) * n_total, true}});
     eigenvalues.resize(n_total);
     int nconv = 0;
-    ctx_->check(trl_cuda_small_eigen(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
-                                     static_cast<double*>(evals_dev_.get()), eigenvectors->data(), eigenvalues.data(), &nconv),
-                "solve_small_dense");
+    if (full_eigenvectors_) {
+      ctx_->check(trl_cuda_small_eigen(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
+                                       static_cast<double*>(evals_dev_.get()), eigenvectors->data(), eigenvalues.data(), &nconv),
+                  "solve_small_dense");
+    }
+    else {
+      // the driver reads the eigenvectors of the kept blocks only (lanczos.hh:105-131)
+      const std::size_t kvec = std::min(n_total, std::max((nev / blocksize + 1) * blocksize, min_eigenvectors_));
+      ctx_->check(trl_cuda_small_eigen_partial(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
+                                               static_cast<int>(kvec), static_cast<double*>(evals_dev_.get()), eigenvectors->data(), eigenvalues.data(), &nconv),
+                  "solve_small_dense");
+    }
     return static_cast<std::size_t>(nconv);
   }
 
@@ -107,6 +117,14 @@ public:
 
   /// Number of Cholesky-QR passes in orthonormalize (2 = CholQR2, 1 = reference CholQR).
   void set_cholqr_passes(int p) { cholqr_passes_ = p; }
+
+  /// true: every eigenvector of the projected problem (cuSOLVER syevd), as the reference's
+  /// dense solver computes; false (default): those of the kept blocks only
+  /// (trl_cuda_small_eigen_partial), all the driver reads.
+  void set_full_eigenvectors(bool on) { full_eigenvectors_ = on; }
+  /// Eigenvectors the partial solve forms at least (a caller that forms more Ritz vectors
+  /// from the last projected problem than the restart keeps).
+  void set_min_eigenvectors(std::size_t k) { min_eigenvectors_ = k; }
   int cholqr_passes() const { return cholqr_passes_; }
 
   /// Classical Gram-Schmidt of w against the `count` contiguous blocks starting at V0
@@ -144,6 +162,8 @@ protected:
 
   Scalar tolerance_ = 1e-8;
   int cholqr_passes_ = 2;
+  bool full_eigenvectors_ = false;
+  std::size_t min_eigenvectors_ = 0;
 };
 
 } // namespace trl::cuda

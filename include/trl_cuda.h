@@ -257,6 +257,15 @@ int trl_cuda_mb_set_diagonal(trl_cuda_handle h, double* dst, const double* host_
  * host_evals (N doubles) a host copy of evals; *host_nconv the number of the first
  * min(nev, N) pairs whose Ritz estimate ||beta y_last|| / max(|theta|, eps) < tol.
  * Synchronises the stream. */
+/* trl_cuda_small_eigen with eigenvectors for the first kvec pairs only (0 <= kvec <= N):
+ * columns kvec.. of evecs are zero; evals, host_evals and *host_nconv (over the first
+ * min(nev, kvec) pairs) as above. The driver reads only the kept kr = nev/bs + 1 blocks of
+ * eigenvectors (lanczos.hh:105-131), so EVPBase::solve_small_dense asks for kr*bs. For
+ * 3 <= N <= 448 and kvec <= 128 it runs on hand-written kernels: Householder
+ * tridiagonalisation in one thread-block cluster, bisection, inverse iteration, and the
+ * back-transform; otherwise it uses trl_cuda_small_eigen. Synchronises the stream. */
+int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, int nblk, int bs, const double* beta, int nev, double tol, int kvec, double* evals,
+                                 double* evecs, double* host_evals, int* host_nconv);
 int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, const double* beta, int nev, double tol, double* evals, double* evecs,
                          double* host_evals, int* host_nconv);
 

@@ -58,6 +58,8 @@ typedef struct trl_solve_params {
   unsigned fp32_ncv;             /* TRL_MODE_MIXED: basis size of the FP32 phase (0: ncv) */
   int refine_fp32;               /* TRL_REFINE_CHEBYSHEV: filter in FP32 while the residual is
                                     above ~2e-5, then in FP64 (0: FP64 only) */
+  int small_eigen_full;          /* 1: every eigenvector of the projected problem (cuSOLVER
+                                    syevd); 0: the kept blocks' only (trl_cuda_small_eigen_partial) */
 } trl_solve_params;
 
 typedef struct trl_solve_info {

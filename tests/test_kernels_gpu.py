@@ -323,6 +323,107 @@ def test_small_eigen_matches_reference(cuda_handle, oracle, bs, nblk):
     assert nconv == nc_ref
 
 
+def _block_layout(D, bs, rng=None):
+    """Dense symmetric D as a block matrix; the upper triangle is overwritten with garbage
+    (both eigensolvers read the lower one)."""
+    N = D.shape[0]
+    nblk = N // bs
+    M = D.copy()
+    if rng is not None:
+        iu = np.triu_indices(N, 1)
+        M[iu] = rng.standard_normal(iu[0].size)
+    return M.reshape(nblk, bs, nblk, bs).transpose(0, 2, 1, 3).copy()
+
+
+def _spectrum_matrix(lam, rng):
+    N = lam.size
+    Q, _ = np.linalg.qr(rng.standard_normal((N, N)))
+    return (Q * lam) @ Q.T
+
+
+def _partial_cases():
+    rng = np.random.default_rng(2024)
+    cases = []
+    for N, bs in ((40, 8), (160, 4), (384, 8), (448, 16)):
+        M = rng.standard_normal((N, N))
+        cases.append((f"random{N}", M + M.T, bs))
+    # exact degenerate pairs and a tight cluster at the wanted end (relative gaps 1e-9)
+    lam = np.linspace(-3.0, 1.0, 384)
+    lam[-1] = lam[-2] = 5.0
+    lam[-10:-2] = 4.0 + 1e-9 * np.arange(8)
+    cases.append(("clustered384", _spectrum_matrix(lam, rng), 8))
+    # a thick-restart projected matrix: kept Ritz values on the diagonal, coupling to the
+    # next block, block-tridiagonal below (the structure lanczos.hh:119-150 builds)
+    bs, nblk, kr = 8, 48, 5
+    N = nblk * bs
+    T = np.zeros((N, N))
+    T[: kr * bs, : kr * bs] = np.diag(np.sort(rng.uniform(440, 444, kr * bs))[::-1])
+    for b in range(kr, nblk):
+        D = rng.standard_normal((bs, bs)) * 50 + np.eye(bs) * 200
+        T[b * bs:(b + 1) * bs, b * bs:(b + 1) * bs] = D + D.T
+        if b + 1 < nblk:
+            Bt = np.triu(rng.standard_normal((bs, bs))) * 20
+            T[(b + 1) * bs:(b + 2) * bs, b * bs:(b + 1) * bs] = Bt
+            T[b * bs:(b + 1) * bs, (b + 1) * bs:(b + 2) * bs] = Bt.T
+    C = rng.standard_normal((bs, kr * bs)) * 1e-3
+    T[kr * bs:(kr + 1) * bs, : kr * bs] = C
+    T[: kr * bs, kr * bs:(kr + 1) * bs] = C.T
+    cases.append(("restart384", T, bs))
+    return cases
+
+
+@pytest.mark.parametrize("case", _partial_cases(), ids=lambda c: c[0])
+def test_small_eigen_partial_matches_full(cuda_handle, oracle, case):
+    """The kept-vectors eigensolver (cluster tridiagonalisation, bisection, inverse iteration)
+    against cuSOLVER's full syevd path and the oracle: all eigenvalues, the first kvec
+    eigenvectors (residual, orthogonality, and the spanned subspace of each cluster), the
+    zeroed remaining columns, and the convergence count."""
+    name, D, bs = case
+    rng = np.random.default_rng(7)
+    N = D.shape[0]
+    T = _block_layout(D, bs, rng)
+    beta = np.triu(rng.standard_normal((bs, bs))) * 1e-9
+    nev = 2 * bs
+    kvec = min(N, (nev // bs + 1) * bs)
+    ev_ref, Y_ref, nc_ref = oracle.solve_small_dense(T, beta, bs, nev, tol=1e-7)
+    for rep in range(2):  # the second call runs on the workspace the first one left
+        evals, evecs, hev, nconv = cuda_handle.small_eigen_partial(dev(T), dev(beta), nev, 1e-7, kvec)
+        nrm = np.abs(ev_ref).max()
+        assert np.allclose(hev, ev_ref, rtol=0, atol=1e-12 * nrm)
+        assert np.array_equal(host(evals), hev)
+        Yg = host(evecs).transpose(0, 2, 1, 3).reshape(N, N)
+        X = Yg[:, :kvec]
+        assert np.all(Yg[:, kvec:] == 0.0)
+        # residual and orthogonality of the returned vectors
+        R = D @ X - X * hev[:kvec]
+        assert np.abs(R).max() < 1e-11 * nrm, np.abs(R).max() / nrm
+        assert np.abs(X.T @ X - np.eye(kvec)).max() < 1e-11
+        # same invariant subspaces as the reference: clusters of eigenvalues closer than
+        # 1e-6 ||T|| compared as subspaces
+        Xr = Y_ref.transpose(0, 2, 1, 3).reshape(N, N)[:, :kvec]
+        c0 = 0
+        while c0 < kvec:
+            c1 = c0 + 1
+            while c1 < kvec and abs(ev_ref[c1] - ev_ref[c1 - 1]) < 1e-6 * nrm:
+                c1 += 1
+            if c1 == kvec and c1 < N and abs(ev_ref[c1] - ev_ref[c1 - 1]) < 1e-6 * nrm:
+                break  # the last cluster continues past kvec: its span is not determined by kvec columns
+            s = np.linalg.svd(Xr[:, c0:c1].T @ X[:, c0:c1], compute_uv=False)
+            assert s.min() > 1 - 1e-9, (name, c0, c1, s.min())
+            c0 = c1
+        assert nconv == nc_ref
+        full = cuda_handle.small_eigen(dev(T), dev(beta), nev, 1e-7)
+        assert np.allclose(hev, full[2], rtol=0, atol=1e-12 * nrm)
+
+
+def test_small_eigen_partial_rejects_bad_kvec(cuda_handle):
+    T = torch.zeros((4, 4, 4, 4), dtype=torch.float64, device="cuda")
+    beta = torch.zeros((4, 4), dtype=torch.float64, device="cuda")
+    with pytest.raises(native.TrlError) as e:
+        cuda_handle.small_eigen_partial(T, beta, 4, 1e-8, 17)
+    assert e.value.status == native.TRL_EINVAL
+
+
 def test_sddmm_matches_dense(cuda_handle):
     rng = np.random.default_rng(11)
     A = _random_csr(3001, rng)

@@ -135,6 +135,22 @@ def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine, refine_fp32)
         assert out["refine_rounds"] == 0 and out["restarts"] > 0
 
 
+@pytest.mark.parametrize("mode", [native.TRL_MODE_FP64, native.TRL_MODE_MIXED])
+def test_partial_and_full_projected_eigensolvers_agree(cfg1_oracle, mode):
+    """The restart's projected eigenproblem solved for the kept eigenvectors only (cluster
+    tridiagonalisation + inverse iteration, the default) and for all of them (cuSOLVER
+    syevd): same eigenpairs, same number of restarts."""
+    A, X0, ref = cfg1_oracle
+    kw = dict(bs=4, nev=10, ncv=160, tol=1e-10, mode=mode, fp32_tol=1e-4)
+    part = native.solve_csr_host(A, X0, small_eigen_full=0, **kw)
+    full = native.solve_csr_host(A, X0, small_eigen_full=1, **kw)
+    assert part["converged"] and full["converged"]
+    assert np.max(np.abs(part["evals"] - full["evals"]) / np.abs(full["evals"])) < 1e-12
+    assert abs(part["restarts"] - full["restarts"]) <= 1 and abs(part["restarts_fp32"] - full["restarts_fp32"]) <= 1
+    assert part["max_theta_residual"] < 1e-10
+    assert max_principal_sine(part["evecs"], ref["ritz"], part["evals"]) < 1e-5
+
+
 @pytest.mark.parametrize("fp32_ncv", [0, 96])
 def test_mixed_loose_fp32_phase_filters_in_fp32(cfg1_oracle, fp32_ncv):
     """A loose FP32 phase (fp32_tol 1e-2, optionally on a smaller FP32 basis) leaves most of

@@ -8,6 +8,7 @@
 // counted on the device. Only the eigenvalues and the converged count come back to the host.
 #include "common.cuh"
 
+#include <cooperative_groups.h>
 #include <cusolverDn.h>
 
 #include <cfloat>
@@ -252,3 +253,629 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
 }
 
 } // extern "C"
+
+// ---- the projected eigenproblem for the eigenvectors the restart keeps ------------------
+//
+// trl_cuda_small_eigen_partial returns every eigenvalue but only the first kvec eigenvectors
+// (|theta| descending), which is all the driver reads (the kept blocks, lanczos.hh:105-131).
+// For 3 <= N <= kTriMaxN and kvec <= kTriMaxVec it runs without cuSOLVER:
+//  1. k_tridiag: Householder tridiagonalisation Q^T A Q = T in ONE thread-block cluster of
+//     kTriC CTAs. A (full symmetric storage) is distributed over the CTAs' shared memory by
+//     rows (row g on CTA g % kTriC); each step exchanges the Householder column and the
+//     vector p = tau A v through distributed shared memory, two cluster barriers per step.
+//     (cuSOLVER's tridiagonalisation of the same matrix is a sequence of small kernels, about
+//     3.7 ms at N = 384 on B200.)
+//  2. k_bisect: all eigenvalues of T by bisection on Sturm counts, one warp per eigenvalue,
+//     each lane evaluating one of 32 points of the interval per iteration (multisection).
+//  3. k_tri_factor / k_tri_solve / k_tri_gs: eigenvectors of T for the kvec selected
+//     eigenvalues by inverse iteration (partial-pivoting LU of T - lambda I, tiny pivots
+//     replaced by eps * ||T||), all vectors at once, then classical Gram-Schmidt applied
+//     twice in ascending eigenvalue order. A solve shrinks the component along an eigenvalue
+//     at distance g by eps * ||T|| / g relative to the wanted one, so three solves separate
+//     every pair with g above ~1e-10 ||T|| to working accuracy; closer pairs (and exactly
+//     equal ones) span their eigenspace and the Gram-Schmidt step makes them orthonormal.
+//     The wanted end of a Lanczos T is one tight cluster (48 values within 5e-4 ||T|| at the
+//     96^3 workload), so vectors are not iterated one after another.
+//  4. k_backtransform: x = Q z, one warp per vector applying the stored reflectors.
+// Otherwise it falls back to trl_cuda_small_eigen and zeroes the columns from kvec on.
+
+namespace {
+
+constexpr int kTriC = 8;           // CTAs in the tridiagonalisation cluster (portable size)
+constexpr int kTriThreads = 512;
+constexpr int kTriMaxN = 448;      // rows per CTA * N * 8 B must fit one CTA's shared memory
+constexpr int kTriMaxVec = 128;    // vectors by inverse iteration
+constexpr int kTriIters = 3;       // inverse-iteration sweeps
+constexpr int kBisectMaxN = kTriMaxN;
+constexpr size_t kTriGsMaxBytes = 200 * 1024; // the K vectors of N entries in one CTA's shared memory
+
+size_t tridiag_smem(int N)
+{
+  const int RB = (N + kTriC - 1) / kTriC;
+  return sizeof(double) * (static_cast<size_t>(RB) * N + 4 * N + 2 * kTriC * (kTriThreads / 32) + 8);
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block sum over kTriThreads threads; `red` holds 32 doubles; all threads get the result
+__device__ double block_sum(double v, double* red)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads(); // red may still be read from a previous call
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (warp == 0) {
+    s = lane < static_cast<int>(blockDim.x >> 5) ? red[lane] : 0.0;
+    s = warp_sum(s);
+    if (lane == 0) red[0] = s;
+  }
+  __syncthreads();
+  return red[0];
+}
+
+// A: N x N symmetric (full storage). Outputs: d[N], e[N-1] of T = Q^T A Q with
+// Q = H_0 ... H_{N-3}, H_k = I - tau_k v_k v_k^T, v_k stored in refl[k*N + k+1 .. N-1]
+// (refl[k*N + k+1] = 1).
+// Exchange by pushing: before each cluster barrier every CTA stores its entries of the
+// Householder column (then of p = tau A v) and its per-warp partial sums into the shared
+// memory of every CTA of the cluster (st.shared::cluster through map_shared_rank); after
+// the barrier each CTA reads only its own shared memory. Every CTA reduces the same
+// partials in the same order, so all hold bit-identical scalars. A buffer filled at one
+// barrier is read before the next one, which its next writers wait for.
+__global__ void __cluster_dims__(kTriC, 1, 1) __launch_bounds__(kTriThreads, 1)
+    k_tridiag(const double* __restrict__ A, int N, double* __restrict__ dout, double* __restrict__ eout, double* __restrict__ tau_out, double* __restrict__ refl)
+{
+  namespace cg = cooperative_groups;
+  constexpr int NW = kTriThreads / 32;
+  constexpr int NP = kTriC * NW; // partials per exchange
+  static_assert(NP == 128, "partials are reduced as 4 per lane");
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = static_cast<int>(cluster.block_rank());
+  const int RB = (N + kTriC - 1) / kTriC;
+  extern __shared__ __align__(16) double sm[];
+  double* rows = sm;              // RB x N, local row l = global row r + kTriC * l
+  double* xfull = rows + RB * N;  // N: column k below the diagonal (pushed by the owners)
+  double* pfull = xfull + N;      // N: p (pushed by the owners)
+  double* vfull = pfull + N;      // N
+  double* wfull = vfull + N;      // N
+  double* part = wfull + N;       // NP sums of squares (slot rank * NW + warp), then x0
+  double* part2 = part + NP + 8;  // NP partial p.v
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  auto local_sum = [&](const double* slot) {
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s += slot[lane + 32 * q];
+    return warp_sum(s);
+  };
+  // store v at offset `at` of `buf` in every CTA of the cluster
+  auto push = [&](double* buf, int at, double v) {
+#pragma unroll
+    for (int q = 0; q < kTriC; ++q) cluster.map_shared_rank(buf, q)[at] = v;
+  };
+
+  for (int idx = tid; idx < RB * N; idx += kTriThreads) {
+    const int l = idx / N, j = idx % N, g = r + kTriC * l;
+    rows[idx] = g < N ? A[static_cast<size_t>(g) * N + j] : 0.0;
+  }
+  cluster.sync(); // every CTA is running before any pushes into it
+
+  for (int k = 0; k < N - 2; ++k) {
+    const int l0 = (k + 1 - r + kTriC - 1) / kTriC > 0 ? (k + 1 - r + kTriC - 1) / kTriC : 0; // first local row > k
+    if (r == k % kTriC && tid == 0) dout[k] = rows[(k / kTriC) * N + k];
+    // ---- phase A: push this CTA's entries of x = A[k+1:, k] and its partial sum of squares
+    {
+      double ssq = 0.0;
+      if (tid < RB - l0) {
+        const int l = l0 + tid, g = r + kTriC * l;
+        if (g < N) {
+          const double x = rows[l * N + k];
+          push(xfull, g, x);
+          if (g > k + 1) ssq = x * x;
+        }
+      }
+      ssq = warp_sum(ssq);
+      if (lane < kTriC) cluster.map_shared_rank(part, lane)[r * NW + warp] = ssq;
+      if (tid == 0 && r == (k + 1) % kTriC) push(part, NP, rows[((k + 1) / kTriC) * N + k]);
+    }
+    cluster.sync(); // #1
+    const double xnorm2 = local_sum(part);
+    const double x0 = part[NP];
+    double tau = 0.0, beta = x0, scale = 0.0;
+    if (xnorm2 > 0.0) {
+      beta = -copysign(sqrt(x0 * x0 + xnorm2), x0);
+      tau = (beta - x0) / beta;
+      scale = 1.0 / (x0 - beta);
+    }
+    for (int j = k + 1 + tid; j < N; j += kTriThreads) vfull[j] = (j == k + 1) ? 1.0 : xfull[j] * scale;
+    __syncthreads();
+    if (r == k % kTriC) {
+      for (int j = k + 1 + tid; j < N; j += kTriThreads) refl[static_cast<size_t>(k) * N + j] = vfull[j];
+      if (tid == 0) {
+        tau_out[k] = tau;
+        eout[k] = beta;
+      }
+    }
+    // ---- phase C: p = tau * A_trail v for this CTA's rows (warp per row), pushed with the
+    // partial p.v
+    double pv = 0.0;
+    for (int l = l0 + warp; l < RB; l += NW) {
+      const int g = r + kTriC * l;
+      if (g >= N) break;
+      double s = 0.0;
+      for (int j = k + 1 + lane; j < N; j += 32) s = fma(rows[l * N + j], vfull[j], s);
+      s = warp_sum(s) * tau;
+      if (lane < kTriC) cluster.map_shared_rank(pfull, lane)[g] = s;
+      pv = fma(s, vfull[g], pv);
+    }
+    if (lane < kTriC) cluster.map_shared_rank(part2, lane)[r * NW + warp] = pv;
+    cluster.sync(); // #2
+    const double K = 0.5 * tau * local_sum(part2);
+    for (int j = k + 1 + tid; j < N; j += kTriThreads) wfull[j] = pfull[j] - K * vfull[j];
+    __syncthreads();
+    // ---- phase D: rank-2 update of this CTA's trailing rows (warp per row)
+    if (tau != 0.0) {
+      for (int l = l0 + warp; l < RB; l += NW) {
+        const int g = r + kTriC * l;
+        if (g >= N) break;
+        const double vg = vfull[g], wg = wfull[g];
+        for (int j = k + 1 + lane; j < N; j += 32) rows[l * N + j] -= vg * wfull[j] + wg * vfull[j];
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (N >= 2 && r == (N - 2) % kTriC) dout[N - 2] = rows[((N - 2) / kTriC) * N + N - 2];
+    if (r == (N - 1) % kTriC) {
+      dout[N - 1] = rows[((N - 1) / kTriC) * N + N - 1];
+      if (N >= 2) eout[N - 2] = rows[((N - 1) / kTriC) * N + N - 2];
+    }
+  }
+  cluster.sync(); // no CTA leaves while another may still store into its shared memory
+}
+
+// number of eigenvalues of the tridiagonal (d, e2 = e^2) below sigma
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int N, double sigma, double pivmin)
+{
+  double q = d[0] - sigma;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = q < 0.0;
+  for (int j = 1; j < N; ++j) {
+    q = (d[j] - sigma) - e2[j - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q < 0.0;
+  }
+  return c;
+}
+
+// w[i] = i-th smallest eigenvalue of the tridiagonal (d, e); one warp per eigenvalue
+__global__ void __launch_bounds__(256) k_bisect(const double* __restrict__ dg, const double* __restrict__ eg, int N, double* __restrict__ w)
+{
+  __shared__ double d[kBisectMaxN], e2[kBisectMaxN];
+  __shared__ double bounds[3];
+  for (int j = threadIdx.x; j < N; j += blockDim.x) {
+    d[j] = dg[j];
+    e2[j] = j + 1 < N ? eg[j] * eg[j] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double lo = d[0], hi = d[0], emax = 0.0;
+    for (int j = 0; j < N; ++j) {
+      const double rad = (j > 0 ? sqrt(e2[j - 1]) : 0.0) + (j + 1 < N ? sqrt(e2[j]) : 0.0);
+      lo = fmin(lo, d[j] - rad);
+      hi = fmax(hi, d[j] + rad);
+      if (j + 1 < N) emax = fmax(emax, e2[j]);
+    }
+    const double nrm = fmax(fabs(lo), fabs(hi));
+    bounds[0] = lo - 2.0 * DBL_EPSILON * nrm * N - DBL_MIN;
+    bounds[1] = hi + 2.0 * DBL_EPSILON * nrm * N + DBL_MIN;
+    bounds[2] = DBL_MIN * fmax(1.0, emax); // pivmin
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= N) return;
+  double lo = bounds[0], hi = bounds[1];
+  const double pivmin = bounds[2];
+  for (int it = 0; it < 64; ++it) {
+    const double width = hi - lo;
+    if (width <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + 2.0 * pivmin) break;
+    const double sigma = lo + width * (lane + 1) / 33.0;
+    const int c = sturm_count(d, e2, N, sigma, pivmin);
+    // smallest lane whose point has more than i eigenvalues below it
+    const unsigned above = __ballot_sync(0xffffffffu, c > i);
+    const int q = above ? __ffs(above) - 1 : 32;
+    const double nlo = q == 0 ? lo : lo + width * q / 33.0;
+    const double nhi = q == 32 ? hi : lo + width * (q + 1) / 33.0;
+    if (!(nhi < hi || nlo > lo)) break; // no progress in floating point
+    lo = nlo;
+    hi = nhi;
+  }
+  if (lane == 0) w[i] = 0.5 * (lo + hi);
+}
+
+__device__ __forceinline__ double hash_unit(unsigned a, unsigned b)
+{
+  unsigned x = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
+  x ^= x >> 15;
+  x *= 0x2C1B3C6Du;
+  x ^= x >> 12;
+  x *= 0x297A2D39u;
+  x ^= x >> 15;
+  return (static_cast<double>(x) / 4294967295.0) * 2.0 - 1.0;
+}
+
+// Inverse iteration for the eigenvectors of the tridiagonal (d, e) at the K eigenvalues
+// w[sel[t]] (sel ascending). Vectors: Z[t * N + i]. Per vector t the factorisation
+// P L U = T - lambda_t I (general tridiagonal LU with partial pivoting; pivots below
+// eps * ||T|| replaced by +-eps * ||T||) is stored as F[t][5][N]: multipliers, 1 / U diagonal,
+// U first and second superdiagonal, pivot flags. The recurrences are sequential: one lane
+// runs them on the vector's shared-memory copy.
+constexpr int kFactorRows = 5;
+
+__global__ void __launch_bounds__(32) k_tri_factor(const double* __restrict__ dg, const double* __restrict__ eg, int N, const double* __restrict__ w, const int* __restrict__ sel,
+                                                   double* __restrict__ F, double* __restrict__ Z)
+{
+  extern __shared__ __align__(16) double fs[]; // 5 x N
+  const int t = blockIdx.x, lane = threadIdx.x;
+  // ||T||_inf (Gershgorin) for the pivot floor
+  double nrm = 0.0;
+  for (int i = lane; i < N; i += 32) nrm = fmax(nrm, fabs(dg[i]) + (i > 0 ? fabs(eg[i - 1]) : 0.0) + (i + 1 < N ? fabs(eg[i]) : 0.0));
+  for (int o = 16; o > 0; o >>= 1) nrm = fmax(nrm, __shfl_xor_sync(0xffffffffu, nrm, o));
+  if (!(nrm > 0.0)) nrm = 1.0;
+  double* DL = fs;
+  double* D = fs + N;
+  double* DU = fs + 2 * N;
+  double* DU2 = fs + 3 * N;
+  double* PV = fs + 4 * N;
+  const double lam = w[sel[t]];
+  for (int i = lane; i < N; i += 32) {
+    D[i] = dg[i] - lam;
+    DL[i] = i + 1 < N ? eg[i] : 0.0;
+    DU[i] = i + 1 < N ? eg[i] : 0.0;
+    DU2[i] = 0.0;
+    PV[i] = 0.0;
+    Z[static_cast<size_t>(t) * N + i] = hash_unit(static_cast<unsigned>(t), static_cast<unsigned>(i));
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const double tiny = DBL_EPSILON * nrm;
+    for (int i = 0; i + 1 < N; ++i) {
+      if (fabs(D[i]) >= fabs(DL[i])) {
+        if (fabs(D[i]) < tiny) D[i] = D[i] < 0.0 ? -tiny : tiny;
+        const double fact = DL[i] / D[i];
+        DL[i] = fact;
+        D[i + 1] -= fact * DU[i];
+      }
+      else {
+        const double fact = D[i] / DL[i];
+        D[i] = DL[i];
+        DL[i] = fact;
+        const double temp = DU[i];
+        DU[i] = D[i + 1];
+        D[i + 1] = temp - fact * D[i + 1];
+        if (i + 2 < N) {
+          DU2[i] = DU[i + 1];
+          DU[i + 1] = -fact * DU[i + 1];
+        }
+        PV[i] = 1.0;
+      }
+    }
+    if (fabs(D[N - 1]) < tiny) D[N - 1] = D[N - 1] < 0.0 ? -tiny : tiny;
+    for (int i = 0; i < N; ++i) D[i] = 1.0 / D[i];
+  }
+  __syncwarp();
+  for (int idx = lane; idx < kFactorRows * N; idx += 32) F[static_cast<size_t>(t) * kFactorRows * N + idx] = fs[idx];
+}
+
+// z_t <- (T - lambda_t I)^{-1} z_t, scaled to unit max-norm
+__global__ void __launch_bounds__(32) k_tri_solve(int N, const double* __restrict__ F, double* __restrict__ Z)
+{
+  extern __shared__ __align__(16) double fs[]; // 5 x N factors, N vector
+  const int t = blockIdx.x, lane = threadIdx.x;
+  for (int idx = lane; idx < kFactorRows * N; idx += 32) fs[idx] = F[static_cast<size_t>(t) * kFactorRows * N + idx];
+  double* x = fs + kFactorRows * N;
+  for (int i = lane; i < N; i += 32) x[i] = Z[static_cast<size_t>(t) * N + i];
+  __syncwarp();
+  if (lane == 0) {
+    const double* DL = fs;
+    const double* RD = fs + N;
+    const double* DU = fs + 2 * N;
+    const double* DU2 = fs + 3 * N;
+    const double* PV = fs + 4 * N;
+    double xi = x[0];
+    for (int i = 0; i + 1 < N; ++i) { // apply P and L, carrying x[i] in a register
+      const double xn = x[i + 1];
+      if (PV[i] == 0.0) {
+        x[i] = xi;
+        xi = xn - DL[i] * xi;
+      }
+      else {
+        x[i] = xn;
+        xi = xi - DL[i] * xn;
+      }
+    }
+    x[N - 1] = xi;
+    double x1 = x[N - 1] * RD[N - 1]; // x[i+1]
+    x[N - 1] = x1;
+    double x2 = 0.0; // x[i+2]
+    if (N > 1) {
+      const double v = (x[N - 2] - DU[N - 2] * x1) * RD[N - 2];
+      x[N - 2] = v;
+      x2 = x1;
+      x1 = v;
+    }
+    for (int i = N - 3; i >= 0; --i) {
+      const double v = (x[i] - DU[i] * x1 - DU2[i] * x2) * RD[i];
+      x[i] = v;
+      x2 = x1;
+      x1 = v;
+    }
+  }
+  __syncwarp();
+  double mx = 0.0;
+  for (int i = lane; i < N; i += 32) mx = fmax(mx, fabs(x[i]));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  const double inv = mx > 0.0 ? 1.0 / mx : 1.0;
+  for (int i = lane; i < N; i += 32) Z[static_cast<size_t>(t) * N + i] = x[i] * inv;
+}
+
+// classical Gram-Schmidt applied twice, column by column in ascending eigenvalue order, on
+// the K vectors held in shared memory; one CTA of kTriThreads threads
+__global__ void __launch_bounds__(kTriThreads) k_tri_gs(int N, int K, double* __restrict__ Z)
+{
+  extern __shared__ __align__(16) double zs[]; // K x N
+  __shared__ double coef[kTriMaxVec];
+  __shared__ double red[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kTriThreads / 32;
+  for (int idx = tid; idx < K * N; idx += kTriThreads) zs[idx] = Z[idx];
+  __syncthreads();
+  for (int j = 0; j < K; ++j) {
+    double* zj = zs + static_cast<size_t>(j) * N;
+    for (int pass = 0; pass < 2 && j > 0; ++pass) {
+      for (int i = warp; i < j; i += NW) {
+        const double* zi = zs + static_cast<size_t>(i) * N;
+        double s = 0.0;
+        for (int n = lane; n < N; n += 32) s = fma(zi[n], zj[n], s);
+        s = warp_sum(s);
+        if (lane == 0) coef[i] = s;
+      }
+      __syncthreads();
+      for (int n = tid; n < N; n += kTriThreads) {
+        double v = zj[n];
+        for (int i = 0; i < j; ++i) v = fma(-coef[i], zs[static_cast<size_t>(i) * N + n], v);
+        zj[n] = v;
+      }
+      __syncthreads();
+    }
+    double s = 0.0;
+    for (int n = tid; n < N; n += kTriThreads) s = fma(zj[n], zj[n], s);
+    s = block_sum(s, red);
+    const double inv = s > 0.0 ? 1.0 / sqrt(s) : 0.0;
+    for (int n = tid; n < N; n += kTriThreads) zj[n] *= inv;
+    __syncthreads();
+  }
+  for (int idx = tid; idx < K * N; idx += kTriThreads) Z[idx] = zs[idx];
+}
+
+// X[t*N + i] = (Q z_t)_i, Q = H_0 ... H_{N-3}; one warp per vector, reflectors staged in
+// shared memory kBtRows at a time (all warps of the CTA share them)
+constexpr int kBtRows = 16;
+
+__global__ void __launch_bounds__(256) k_backtransform(const double* __restrict__ Z, int K, int N, const double* __restrict__ tau, const double* __restrict__ refl,
+                                                       double* __restrict__ X)
+{
+  constexpr int PER = (kTriMaxN + 31) / 32;
+  extern __shared__ __align__(16) double vs[]; // kBtRows x N
+  __shared__ double ts[kBtRows];
+  const int lane = threadIdx.x & 31;
+  const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const bool active = t < K;
+  double z[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int i = lane + 32 * q;
+    z[q] = (active && i < N) ? Z[static_cast<size_t>(t) * N + i] : 0.0;
+  }
+  for (int khi = N - 3; khi >= 0; khi -= kBtRows) {
+    const int klo = khi - kBtRows + 1 > 0 ? khi - kBtRows + 1 : 0;
+    __syncthreads(); // the previous chunk is no longer read
+    for (int idx = threadIdx.x; idx < (khi - klo + 1) * N; idx += blockDim.x) {
+      const int rr = idx / N, i = idx % N;
+      vs[rr * N + i] = refl[static_cast<size_t>(klo + rr) * N + i];
+    }
+    if (threadIdx.x <= khi - klo) ts[threadIdx.x] = tau[klo + threadIdx.x];
+    __syncthreads();
+    if (active) {
+      for (int k = khi; k >= klo; --k) {
+        const double tk = ts[k - klo];
+        if (tk == 0.0) continue;
+        const double* v = vs + (k - klo) * N;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+          const int i = lane + 32 * q;
+          if (i > k && i < N) s = fma(v[i], z[q], s);
+        }
+        s = warp_sum(s) * tk;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+          const int i = lane + 32 * q;
+          if (i > k && i < N) z[q] = fma(-s, v[i], z[q]);
+        }
+      }
+    }
+  }
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int i = lane + 32 * q;
+      if (i < N) X[static_cast<size_t>(t) * N + i] = z[q];
+    }
+  }
+}
+
+// selected ascending indices: sel[t] (ascending), slot[c] = t for rank c < K
+__global__ void k_select(const int* __restrict__ perm, int K, int* __restrict__ sel, int* __restrict__ slot)
+{
+  const int c = threadIdx.x;
+  if (c >= K) return;
+  const int a = perm[c];
+  int t = 0;
+  for (int q = 0; q < K; ++q) t += perm[q] < a;
+  sel[t] = a;
+  slot[c] = t;
+}
+
+// Y in block layout: column c < K is X[slot[c]], the rest zero
+__global__ void k_scatter_partial(const double* __restrict__ X, const int* __restrict__ slot, int nblk, int bs, int K, double* __restrict__ Y)
+{
+  const int N = nblk * bs;
+  const int64_t total = static_cast<int64_t>(N) * N;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int cj = static_cast<int>(e % bs);
+    const int64_t q = e / bs;
+    const int ri = static_cast<int>(q % bs);
+    const int64_t blk = q / bs;
+    const int bj = static_cast<int>(blk % nblk), bi = static_cast<int>(blk / nblk);
+    const int row = bi * bs + ri, col = bj * bs + cj;
+    Y[e] = col < K ? X[static_cast<int64_t>(slot[col]) * N + row] : 0.0;
+  }
+}
+
+__global__ void k_count_partial(const double* __restrict__ X, const int* __restrict__ slot, const double* __restrict__ evals_sorted, const double* __restrict__ beta, int nblk, int bs,
+                                int ncheck, double tol, int* __restrict__ count)
+{
+  const int N = nblk * bs;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncheck; c += gridDim.x * blockDim.x) {
+    const double* y = X + static_cast<int64_t>(slot[c]) * N + (nblk - 1) * bs;
+    double nrm2 = 0.0;
+    for (int i = 0; i < bs; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < bs; ++k) s += beta[i * bs + k] * y[k];
+      nrm2 += s * s;
+    }
+    const double denom = fmax(fabs(evals_sorted[c]), DBL_EPSILON);
+    if (sqrt(nrm2) / denom < tol) atomicAdd(count, 1);
+  }
+}
+
+// zero the block-layout columns >= K of Y
+__global__ void k_zero_cols(double* __restrict__ Y, int nblk, int bs, int K)
+{
+  const int N = nblk * bs;
+  const int64_t total = static_cast<int64_t>(N) * N;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int cj = static_cast<int>(e % bs);
+    const int bj = static_cast<int>((e / (static_cast<int64_t>(bs) * bs)) % nblk);
+    if (bj * bs + cj >= K) Y[e] = 0.0;
+  }
+}
+
+} // namespace
+
+extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, int nblk, int bs, const double* beta, int nev, double tol, int kvec, double* evals, double* evecs,
+                                            double* host_evals, int* host_nconv)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!valid_bs(bs) || nblk <= 0 || !T || !beta || !evals || !evecs || !host_evals || !host_nconv) return set_error(h, TRL_EINVAL, "bad small_eigen arguments");
+  const int N = nblk * bs;
+  if (kvec < 0 || kvec > N) return set_error(h, TRL_EINVAL, "kvec %d outside [0, %d]", kvec, N);
+  static int cluster_ok = -1; // whether a kTriC-CTA cluster with the shared memory of N = kTriMaxN can be resident
+  if (cluster_ok < 0) {
+    cluster_ok = 0;
+    const size_t smem = tridiag_smem(kTriMaxN);
+    if (cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_tri_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTriGsMaxBytes)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * kBtRows * kTriMaxN)) == cudaSuccess) {
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(kTriC);
+      cfg.blockDim = dim3(kTriThreads);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr{};
+      attr.id = cudaLaunchAttributeClusterDimension;
+      attr.val.clusterDim.x = kTriC;
+      attr.val.clusterDim.y = 1;
+      attr.val.clusterDim.z = 1;
+      cfg.attrs = &attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, k_tridiag, &cfg) == cudaSuccess && clusters > 0) cluster_ok = 1;
+    }
+    cudaGetLastError();
+  }
+  if (N < 3 || N > kTriMaxN || kvec > kTriMaxVec || sizeof(double) * N * (kvec > 0 ? kvec : 1) > kTriGsMaxBytes || cluster_ok != 1) {
+    if (int st = trl_cuda_small_eigen(h, T, nblk, bs, beta, nev, tol, evals, evecs, host_evals, host_nconv)) return st;
+    k_zero_cols<<<grid_for(h, static_cast<int64_t>(N) * N, 256, 4), 256, 0, h->stream>>>(evecs, nblk, bs, kvec);
+    return after_launch(h, "zero columns");
+  }
+  ProfScope prof(h, PROF_SMALL_EIGEN, 16.0 * N * N);
+  const int K = kvec > 0 ? kvec : 1;
+  // workspace: A (N*N) | refl (N*N) | d | e | tau | w (N each) | Z (N*K) | X (N*K) |
+  // factors (5 N*K) | perm, sel, slot (N ints each) | zero flag, count
+  const size_t NN = static_cast<size_t>(N) * N, NK = static_cast<size_t>(N) * K;
+  const size_t doubles = 2 * NN + 4 * static_cast<size_t>(N) + (2 + kFactorRows) * NK;
+  const size_t ints = 3 * static_cast<size_t>(N) + 8;
+  char* ws = static_cast<char*>(workspace(h, sizeof(double) * doubles + sizeof(int) * ints + 256));
+  if (!ws) return TRL_ENOMEM;
+  double* A = reinterpret_cast<double*>(ws);
+  double* refl = A + NN;
+  double* d = refl + NN;
+  double* e = d + N;
+  double* tau = e + N;
+  double* w = tau + N;
+  double* Z = w + N;
+  double* X = Z + NK;
+  double* F = X + NK;
+  int* perm = reinterpret_cast<int*>(F + kFactorRows * NK);
+  int* sel = perm + N;
+  int* slot = sel + N;
+  int* flags = slot + N; // [0] = 0 (no solver error), [1] = converged count
+
+  const unsigned g = grid_for(h, static_cast<int64_t>(N) * N, 256, 4);
+  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, A);
+  if (int st = after_launch(h, "assemble")) return st;
+  cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream);
+  k_tridiag<<<kTriC, kTriThreads, tridiag_smem(N), h->stream>>>(A, N, d, e, tau, refl);
+  if (int st = after_launch(h, "tridiagonalise")) return st;
+  k_bisect<<<(N + 7) / 8, 256, 0, h->stream>>>(d, e, N, w);
+  if (int st = after_launch(h, "bisect")) return st;
+  k_rank<<<(N + 255) / 256, 256, 0, h->stream>>>(w, N, perm, evals, flags, h->d_status);
+  if (int st = after_launch(h, "rank")) return st;
+  k_select<<<1, kTriMaxVec, 0, h->stream>>>(perm, K, sel, slot);
+  if (int st = after_launch(h, "select")) return st;
+  k_tri_factor<<<K, 32, sizeof(double) * kFactorRows * N, h->stream>>>(d, e, N, w, sel, F, Z);
+  if (int st = after_launch(h, "tridiagonal factor")) return st;
+  for (int it = 0; it < kTriIters; ++it) {
+    k_tri_solve<<<K, 32, sizeof(double) * (kFactorRows + 1) * N, h->stream>>>(N, F, Z);
+    if (int st = after_launch(h, "inverse iteration")) return st;
+  }
+  k_tri_gs<<<1, kTriThreads, sizeof(double) * NK, h->stream>>>(N, K, Z);
+  if (int st = after_launch(h, "gram-schmidt")) return st;
+  k_backtransform<<<(K + 7) / 8, 256, sizeof(double) * kBtRows * N, h->stream>>>(Z, K, N, tau, refl, X);
+  if (int st = after_launch(h, "back-transform")) return st;
+  k_scatter_partial<<<g, 256, 0, h->stream>>>(X, slot, nblk, bs, kvec, evecs);
+  if (int st = after_launch(h, "scatter")) return st;
+  const int ncheck = nev < kvec ? nev : kvec;
+  if (ncheck > 0) {
+    k_count_partial<<<(ncheck + 127) / 128, 128, 0, h->stream>>>(X, slot, evals, beta, nblk, bs, ncheck, tol, flags + 1);
+    if (int st = after_launch(h, "count")) return st;
+  }
+  const size_t w_bytes = sizeof(double) * N;
+  char* pin = static_cast<char*>(pinned(h, w_bytes + 64));
+  if (!pin) return TRL_ENOMEM;
+  cudaMemcpyAsync(pin, evals, w_bytes, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(pin + w_bytes, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  int st = trl_cuda_synchronize(h);
+  if (st) return st;
+  std::memcpy(host_evals, pin, w_bytes);
+  std::memcpy(host_nconv, pin + w_bytes, sizeof(int));
+  return TRL_OK;
+}

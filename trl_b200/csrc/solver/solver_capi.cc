@@ -85,6 +85,8 @@ PhaseOut run_phase(const std::shared_ptr<Context>& ctx, const trl_csr* A, const 
   auto Adev = DeviceCSR<Storage>::wrap(A->n, A->nnz, A->rowptr, A->colind, static_cast<const Storage*>(A->values));
   auto evp = std::make_shared<EVP>(ctx, std::move(Adev), p.alpha, p.beta);
   evp->set_cholqr_passes(p.cholqr_passes);
+  evp->set_full_eigenvectors(p.small_eigen_full != 0);
+  evp->set_min_eigenvectors(static_cast<std::size_t>(kx) * bs); // the Ritz vectors formed below
   trl::EigensolverParams ep{.nev = p.nev, .ncv = p.ncv, .max_restarts = max_restarts, .tolerance = tol};
   trl::BlockLanczos<EVP, Reorth> lanczos(evp, ep);
   auto V0 = lanczos.initial_block();

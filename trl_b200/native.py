@@ -68,6 +68,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_mb_mult": (C.c_int, [P, P, P, P, C.c_int]),
     "trl_cuda_mb_set_diagonal": (C.c_int, [P, P, P, C.c_int]),
     "trl_cuda_small_eigen": (C.c_int, [P, P, C.c_int, C.c_int, P, C.c_int, C.c_double, P, P, P, C.POINTER(C.c_int)]),
+    "trl_cuda_small_eigen_partial": (C.c_int, [P, P, C.c_int, C.c_int, P, C.c_int, C.c_double, C.c_int, P, P, P, C.POINTER(C.c_int)]),
     "trl_cuda_profile_enable": (C.c_int, [P, C.c_int]),
     "trl_cuda_profile_read": (C.c_int, [P, P]),
 }
@@ -88,7 +89,7 @@ class trl_solve_params(C.Structure):
                 ("tol", C.c_double), ("alpha", C.c_double), ("beta", C.c_double), ("reorth", C.c_int),
                 ("cholqr_passes", C.c_int), ("fp32_tol", C.c_double), ("refine_max_restarts", C.c_uint),
                 ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint), ("refine", C.c_int),
-                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int)]
+                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int), ("small_eigen_full", C.c_int)]
 
 
 class trl_solve_info(C.Structure):
@@ -281,6 +282,20 @@ class Handle:
         wt = np.ascontiguousarray(weights, dtype=np.float64)
         self.check(self.lib.trl_cuda_eigen_adjoint(self.h, C.byref(pattern.desc), _ptr(X), k, ev.ctypes.data, wt.ctypes.data,
                                                    cluster_rtol, kind, _ptr(grad)))
+
+    def small_eigen_partial(self, T, beta, nev: int, tol: float, kvec: int):
+        """As small_eigen, eigenvectors for the first kvec pairs (|theta| descending) only."""
+        import torch
+
+        nblk, _, bs, _ = T.shape
+        N = nblk * bs
+        evals = torch.empty(N, dtype=torch.float64, device=T.device)
+        evecs = torch.full_like(T, float("nan"))
+        host = np.zeros(N)
+        nconv = C.c_int(0)
+        self.check(self.lib.trl_cuda_small_eigen_partial(self.h, _ptr(T), nblk, bs, _ptr(beta), nev, tol, kvec, _ptr(evals), _ptr(evecs),
+                                                         host.ctypes.data, C.byref(nconv)))
+        return evals, evecs, host, nconv.value
 
     def small_eigen(self, T, beta, nev: int, tol: float):
         """T: block matrix (nblk, nblk, bs, bs) float64 on the device."""
