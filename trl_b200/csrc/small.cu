@@ -276,7 +276,8 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
 //     equal ones) span their eigenspace and the Gram-Schmidt step makes them orthonormal.
 //     The wanted end of a Lanczos T is one tight cluster (48 values within 5e-4 ||T|| at the
 //     96^3 workload), so vectors are not iterated one after another.
-//  4. k_backtransform: x = Q z, one warp per vector applying the stored reflectors.
+//  4. k_wy_factor / k_backtransform: x = Q z with the stored reflectors in compact WY
+//     chunks (Q restricted to a chunk = I - V T V^T).
 // Otherwise it falls back to trl_cuda_small_eigen and zeroes the columns from kvec on.
 
 namespace {
@@ -317,6 +318,28 @@ __device__ double block_sum(double v, double* red)
   }
   __syncthreads();
   return red[0];
+}
+
+// dst[i] = src[i], i < count, by all threads of the CTA with kStageBatch global loads in
+// flight per thread (a plain copy loop waits for each load before its store)
+constexpr int kStageBatch = 8;
+
+__device__ __forceinline__ void stage(double* dst, const double* __restrict__ src, int count)
+{
+  const int step = static_cast<int>(blockDim.x);
+  for (int base = threadIdx.x; base < count; base += step * kStageBatch) {
+    double v[kStageBatch];
+#pragma unroll
+    for (int u = 0; u < kStageBatch; ++u) {
+      const int i = base + u * step;
+      v[u] = i < count ? src[i] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kStageBatch; ++u) {
+      const int i = base + u * step;
+      if (i < count) dst[i] = v[u];
+    }
+  }
 }
 
 // A: N x N symmetric (full storage). Outputs: d[N], e[N-1] of T = Q^T A Q with
@@ -360,9 +383,11 @@ __global__ void __cluster_dims__(kTriC, 1, 1) __launch_bounds__(kTriThreads, 1)
     for (int q = 0; q < kTriC; ++q) cluster.map_shared_rank(buf, q)[at] = v;
   };
 
-  for (int idx = tid; idx < RB * N; idx += kTriThreads) {
-    const int l = idx / N, j = idx % N, g = r + kTriC * l;
-    rows[idx] = g < N ? A[static_cast<size_t>(g) * N + j] : 0.0;
+  for (int l = 0; l < RB; ++l) {
+    const int g = r + kTriC * l;
+    if (g < N) stage(rows + l * N, A + static_cast<size_t>(g) * N, N);
+    else
+      for (int j = tid; j < N; j += kTriThreads) rows[l * N + j] = 0.0;
   }
   cluster.sync(); // every CTA is running before any pushes into it
 
@@ -635,7 +660,7 @@ __global__ void __launch_bounds__(kTriThreads) k_tri_gs(int N, int K, double* __
   __shared__ double red[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = kTriThreads / 32;
-  for (int idx = tid; idx < K * N; idx += kTriThreads) zs[idx] = Z[idx];
+  stage(zs, Z, K * N);
   __syncthreads();
   for (int j = 0; j < K; ++j) {
     double* zj = zs + static_cast<size_t>(j) * N;
@@ -665,61 +690,112 @@ __global__ void __launch_bounds__(kTriThreads) k_tri_gs(int N, int K, double* __
   for (int idx = tid; idx < K * N; idx += kTriThreads) Z[idx] = zs[idx];
 }
 
-// X[t*N + i] = (Q z_t)_i, Q = H_0 ... H_{N-3}; one warp per vector, reflectors staged in
-// shared memory kBtRows at a time (all warps of the CTA share them)
-constexpr int kBtRows = 16;
+// Back-transform X = Q Z, Q = H_0 ... H_{N-3}, in chunks of kWyRows reflectors: a chunk
+// H_a ... H_b equals I - V T V^T (compact WY form, T upper triangular: T_ii = tau_i,
+// T[0:i, i] = -tau_i T[0:i, 0:i] V[:, 0:i]^T v_i), so a chunk is three small matrix
+// products on the vectors instead of kWyRows dependent reflector applications.
+constexpr int kWyRows = 16;
+constexpr int kWyVecs = 1; // vectors per CTA: the chunk products are latency-bound, so one vector per CTA spreads them over K SMs
 
-__global__ void __launch_bounds__(256) k_backtransform(const double* __restrict__ Z, int K, int N, const double* __restrict__ tau, const double* __restrict__ refl,
+// T of chunk c (reflectors c * kWyRows ...) into Tw[c][kWyRows][kWyRows]
+__global__ void __launch_bounds__(256) k_wy_factor(const double* __restrict__ refl, const double* __restrict__ tau, int N, double* __restrict__ Tw)
+{
+  extern __shared__ __align__(16) double vs[]; // kWyRows x N
+  __shared__ double G[kWyRows][kWyRows], Tt[kWyRows][kWyRows];
+  const int R = N - 2;
+  const int k0 = blockIdx.x * kWyRows;
+  const int b = R - k0 < kWyRows ? R - k0 : kWyRows;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  stage(vs, refl + static_cast<size_t>(k0) * N, b * N);
+  __syncthreads();
+  for (int rr = 0; rr < b; ++rr) // v_k is zero up to row k (refl holds nothing there)
+    for (int i = tid; i <= k0 + rr; i += blockDim.x) vs[rr * N + i] = 0.0;
+  __syncthreads();
+  for (int pq = warp; pq < b * b; pq += blockDim.x >> 5) {
+    const int p = pq / b, q = pq % b;
+    if (p >= q) continue; // strictly upper part: G[p][q] = v_p . v_q
+    double s = 0.0;
+    for (int i = lane; i < N; i += 32) s = fma(vs[p * N + i], vs[q * N + i], s);
+    s = warp_sum(s);
+    if (lane == 0) G[p][q] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int i = 0; i < b; ++i) {
+      const double ti = tau[k0 + i];
+      // lane j < i: T[j][i] = -tau_i sum_{m=j}^{i-1} T[j][m] G[m][i]
+      double v = 0.0;
+      if (lane < i) {
+        for (int m = lane; m < i; ++m) v = fma(Tt[lane][m], G[m][i], v);
+        v = -ti * v;
+      }
+      __syncwarp();
+      if (lane < i) Tt[lane][i] = v;
+      if (lane == i) Tt[i][i] = ti;
+      if (lane > i && lane < kWyRows) Tt[lane][i] = 0.0;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < kWyRows * kWyRows; e += blockDim.x) {
+    const int p = e / kWyRows, q = e % kWyRows;
+    Tw[static_cast<size_t>(blockIdx.x) * kWyRows * kWyRows + e] = (p < b && q < b) ? Tt[p][q] : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_backtransform(const double* __restrict__ Z, int K, int N, const double* __restrict__ refl, const double* __restrict__ Tw,
                                                        double* __restrict__ X)
 {
-  constexpr int PER = (kTriMaxN + 31) / 32;
-  extern __shared__ __align__(16) double vs[]; // kBtRows x N
-  __shared__ double ts[kBtRows];
-  const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const bool active = t < K;
-  double z[PER];
-#pragma unroll
-  for (int q = 0; q < PER; ++q) {
-    const int i = lane + 32 * q;
-    z[q] = (active && i < N) ? Z[static_cast<size_t>(t) * N + i] : 0.0;
-  }
-  for (int khi = N - 3; khi >= 0; khi -= kBtRows) {
-    const int klo = khi - kBtRows + 1 > 0 ? khi - kBtRows + 1 : 0;
-    __syncthreads(); // the previous chunk is no longer read
-    for (int idx = threadIdx.x; idx < (khi - klo + 1) * N; idx += blockDim.x) {
-      const int rr = idx / N, i = idx % N;
-      vs[rr * N + i] = refl[static_cast<size_t>(klo + rr) * N + i];
-    }
-    if (threadIdx.x <= khi - klo) ts[threadIdx.x] = tau[klo + threadIdx.x];
+  extern __shared__ __align__(16) double sm[]; // kWyRows x N reflectors | kWyVecs x N vectors
+  double* vs = sm;
+  double* xs = sm + kWyRows * N;
+  __shared__ double W[kWyRows][kWyVecs], W2[kWyRows][kWyVecs], Ts[kWyRows][kWyRows];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t0 = blockIdx.x * kWyVecs;
+  const int nv = K - t0 < kWyVecs ? K - t0 : kWyVecs;
+  stage(xs, Z + static_cast<size_t>(t0) * N, nv * N);
+  const int R = N - 2;
+  const int nch = (R + kWyRows - 1) / kWyRows;
+  for (int c = nch - 1; c >= 0; --c) {
+    const int k0 = c * kWyRows;
+    const int b = R - k0 < kWyRows ? R - k0 : kWyRows;
+    __syncthreads(); // previous chunk done with vs, Ts, W2
+    stage(vs, refl + static_cast<size_t>(k0) * N, b * N);
+    for (int e = tid; e < kWyRows * kWyRows; e += blockDim.x) Ts[e / kWyRows][e % kWyRows] = Tw[static_cast<size_t>(c) * kWyRows * kWyRows + e];
     __syncthreads();
-    if (active) {
-      for (int k = khi; k >= klo; --k) {
-        const double tk = ts[k - klo];
-        if (tk == 0.0) continue;
-        const double* v = vs + (k - klo) * N;
-        double s = 0.0;
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-          const int i = lane + 32 * q;
-          if (i > k && i < N) s = fma(v[i], z[q], s);
-        }
-        s = warp_sum(s) * tk;
-#pragma unroll
-        for (int q = 0; q < PER; ++q) {
-          const int i = lane + 32 * q;
-          if (i > k && i < N) z[q] = fma(-s, v[i], z[q]);
-        }
+    for (int rr = 0; rr < b; ++rr) // v_k is zero up to row k (refl holds nothing there)
+      for (int i = tid; i <= k0 + rr; i += blockDim.x) vs[rr * N + i] = 0.0;
+    __syncthreads();
+    // W = V^T X: warp per (row, vector) pair
+    for (int pv = warp; pv < b * nv; pv += blockDim.x >> 5) {
+      const int rr = pv / nv, v = pv % nv;
+      double s0 = 0.0, s1 = 0.0;
+      int i = lane;
+      for (; i + 32 < N; i += 64) {
+        s0 = fma(vs[rr * N + i], xs[v * N + i], s0);
+        s1 = fma(vs[rr * N + i + 32], xs[v * N + i + 32], s1);
       }
+      if (i < N) s0 = fma(vs[rr * N + i], xs[v * N + i], s0);
+      const double s = warp_sum(s0 + s1);
+      if (lane == 0) W[rr][v] = s;
+    }
+    __syncthreads();
+    if (tid < b * nv) { // W2 = T W
+      const int rr = tid / nv, v = tid % nv;
+      double s = 0.0;
+      for (int m = rr; m < b; ++m) s = fma(Ts[rr][m], W[m][v], s);
+      W2[rr][v] = s;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nv * N; idx += blockDim.x) { // X -= V W2
+      const int v = idx / N, i = idx % N;
+      double x = xs[idx];
+      for (int rr = 0; rr < b; ++rr) x = fma(-vs[rr * N + i], W2[rr][v], x);
+      xs[idx] = x;
     }
   }
-  if (active) {
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const int i = lane + 32 * q;
-      if (i < N) X[static_cast<size_t>(t) * N + i] = z[q];
-    }
-  }
+  __syncthreads();
+  for (int idx = tid; idx < nv * N; idx += blockDim.x) X[static_cast<size_t>(t0) * N + idx] = xs[idx];
 }
 
 // selected ascending indices: sel[t] (ascending), slot[c] = t for rank c < K
@@ -794,7 +870,8 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
     const size_t smem = tridiag_smem(kTriMaxN);
     if (cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) == cudaSuccess &&
         cudaFuncSetAttribute(k_tri_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTriGsMaxBytes)) == cudaSuccess &&
-        cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * kBtRows * kTriMaxN)) == cudaSuccess) {
+        cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * (kWyRows + kWyVecs) * kTriMaxN)) == cudaSuccess &&
+        cudaFuncSetAttribute(k_wy_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * kWyRows * kTriMaxN)) == cudaSuccess) {
       cudaLaunchConfig_t cfg{};
       cfg.gridDim = dim3(kTriC);
       cfg.blockDim = dim3(kTriThreads);
@@ -821,7 +898,8 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   // workspace: A (N*N) | refl (N*N) | d | e | tau | w (N each) | Z (N*K) | X (N*K) |
   // factors (5 N*K) | perm, sel, slot (N ints each) | zero flag, count
   const size_t NN = static_cast<size_t>(N) * N, NK = static_cast<size_t>(N) * K;
-  const size_t doubles = 2 * NN + 4 * static_cast<size_t>(N) + (2 + kFactorRows) * NK;
+  const size_t nchunks = static_cast<size_t>(N - 2 + kWyRows - 1) / kWyRows;
+  const size_t doubles = 2 * NN + 4 * static_cast<size_t>(N) + (2 + kFactorRows) * NK + nchunks * kWyRows * kWyRows;
   const size_t ints = 3 * static_cast<size_t>(N) + 8;
   char* ws = static_cast<char*>(workspace(h, sizeof(double) * doubles + sizeof(int) * ints + 256));
   if (!ws) return TRL_ENOMEM;
@@ -834,7 +912,8 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   double* Z = w + N;
   double* X = Z + NK;
   double* F = X + NK;
-  int* perm = reinterpret_cast<int*>(F + kFactorRows * NK);
+  double* Tw = F + kFactorRows * NK;
+  int* perm = reinterpret_cast<int*>(Tw + nchunks * kWyRows * kWyRows);
   int* sel = perm + N;
   int* slot = sel + N;
   int* flags = slot + N; // [0] = 0 (no solver error), [1] = converged count
@@ -859,7 +938,10 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   }
   k_tri_gs<<<1, kTriThreads, sizeof(double) * NK, h->stream>>>(N, K, Z);
   if (int st = after_launch(h, "gram-schmidt")) return st;
-  k_backtransform<<<(K + 7) / 8, 256, sizeof(double) * kBtRows * N, h->stream>>>(Z, K, N, tau, refl, X);
+  const int nch = (N - 2 + kWyRows - 1) / kWyRows;
+  k_wy_factor<<<nch, 256, sizeof(double) * kWyRows * N, h->stream>>>(refl, tau, N, Tw);
+  if (int st = after_launch(h, "wy factor")) return st;
+  k_backtransform<<<(K + kWyVecs - 1) / kWyVecs, 256, sizeof(double) * (kWyRows + kWyVecs) * N, h->stream>>>(Z, K, N, refl, Tw, X);
   if (int st = after_launch(h, "back-transform")) return st;
   k_scatter_partial<<<g, 256, 0, h->stream>>>(X, slot, nblk, bs, kvec, evecs);
   if (int st = after_launch(h, "scatter")) return st;
