@@ -101,6 +101,16 @@ int trl_solve_csr_device(trl_cuda_handle h, const trl_solve_params* p, const trl
 
 const char* trl_solver_last_error(void);
 
+/* Matrix Market coordinate file -> CSR in full storage, in host memory allocated with
+ * malloc (free with trl_csr_free_host). Replaces the reference's loader
+ * (examples/sycl/csrevp.hh:26-124) with its semantics: a "symmetric" header mirrors every
+ * off-diagonal entry (the mirror right after it), indices are 1-based in the file, entries
+ * of a row keep their order in the file, duplicates are kept. Also reads "integer" and
+ * "pattern" (value 1) files. `threads` host threads parse the data (<= 0: all cores).
+ * TRL_EINVAL on a malformed file (message in trl_solver_last_error). */
+int trl_csr_read_mtx(const char* path, int threads, int64_t* n_rows, int64_t* n_cols, int64_t* nnz, int32_t** rowptr, int32_t** colind, double** values);
+void trl_csr_free_host(int32_t* rowptr, int32_t* colind, double* values);
+
 #ifdef __cplusplus
 }
 #endif

@@ -124,3 +124,51 @@ def symmetric_eigen(A: np.ndarray):
     V = np.zeros((n, n))
     _check(lib().oracle_symmetric_eigen(n, _p(A), _p(w), _p(V)))
     return w, V
+
+
+def read_mtx(path: str):
+    """Restatement of the reference's Matrix Market loader (examples/sycl/csrevp.hh:26-124),
+    in plain Python for small files: header "symmetric" (any case) mirrors each off-diagonal
+    entry right after it (:70-76), 1-based indices (:66-67), row counts and prefix sum
+    (:93-98), then a scatter in reading order (:101-107). Returns (n_rows, n_cols, rowptr,
+    colind, values). Extension read the same way as the library does: "pattern" files take
+    value 1."""
+    symmetric = pattern = False
+    with open(path) as f:
+        lines = f.read().split("\n")
+    i = 0
+    while i < len(lines):
+        s = lines[i].strip()
+        if not s:
+            i += 1
+            continue
+        if s.startswith("%"):
+            low = s.lower()
+            if low.startswith("%%matrixmarket"):
+                symmetric = "symmetric" in low
+                pattern = "pattern" in low
+            i += 1
+            continue
+        break
+    rows, cols, entries = (int(t) for t in lines[i].split()[:3])
+    toks = [t for ln in lines[i + 1:] if not ln.strip().startswith("%") for t in ln.split()]
+    per = 2 if pattern else 3
+    coo = []
+    for e in range(entries):
+        r, c = int(toks[per * e]) - 1, int(toks[per * e + 1]) - 1
+        v = 1.0 if pattern else float(toks[per * e + 2])
+        coo.append((r, c, v))
+        if symmetric and r != c:
+            coo.append((c, r, v))
+    rowptr = np.zeros(rows + 1, dtype=np.int32)
+    for r, _, _ in coo:
+        rowptr[r + 1] += 1
+    rowptr = np.cumsum(rowptr).astype(np.int32)
+    pos = rowptr[:-1].copy()
+    colind = np.zeros(len(coo), dtype=np.int32)
+    values = np.zeros(len(coo))
+    for r, c, v in coo:
+        colind[pos[r]] = c
+        values[pos[r]] = v
+        pos[r] += 1
+    return rows, cols, rowptr, colind, values

@@ -83,10 +83,10 @@ def build_solver(ref: str = DEFAULT_REF, verbose: bool = False) -> list[str]:
     common = [CXX, "-std=c++20", "-O2", "-fPIC", f"-I{INCLUDE}", f"-I{ref_inc}", f"-I{CUDA_HOME}/include"]
     link = [f"-L{LIB}", "-ltrl_cuda", f"-L{CUDA_HOME}/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{CUDA_HOME}/lib64"]
     out = []
-    src = os.path.join(CSRC, "solver", "solver_capi.cc")
+    srcs = [os.path.join(CSRC, "solver", f) for f in ("solver_capi.cc", "mtx.cc")]
     so = os.path.join(LIB, "libtrl_solver.so")
-    if _newer(so, [src, os.path.join(LIB, "libtrl_cuda.so")] + hdrs):
-        _run(common + ["-shared", "-o", so, src] + link, verbose)
+    if _newer(so, srcs + [os.path.join(LIB, "libtrl_cuda.so")] + hdrs):
+        _run(common + ["-shared", "-o", so, *srcs] + link + ["-pthread"], verbose)
     out.append(so)
     src = os.path.join(CSRC, "solver", "ref_tests_cuda.cc")
     exe = os.path.join(LIB, "trl_cuda_ref_tests")

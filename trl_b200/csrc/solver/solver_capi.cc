@@ -569,6 +569,18 @@ int fail(const std::exception& e, int status)
   return status;
 }
 
+} // namespace
+
+namespace trl_solver_detail {
+int set_error(int status, const char* msg)
+{
+  g_err = msg;
+  return status;
+}
+} // namespace trl_solver_detail
+
+namespace {
+
 // trl_solve_csr_host's context on each device: created by the first call and kept until
 // the process exits, so that its memory pool keeps the solve's buffers reserved between
 // calls (allocating and freeing a solve's 4-6 GB each call cost up to a second of host time

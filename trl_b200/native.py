@@ -106,6 +106,9 @@ SOLVER_SYMBOLS = {
     "trl_solve_csr_host": (C.c_int, [C.POINTER(trl_solve_params), C.c_int, I64, I64, P, P, P, P, P, P, P, C.POINTER(trl_solve_info)]),
     "trl_solve_csr_device": (C.c_int, [P, C.POINTER(trl_solve_params), P, P, P, P, P, P, C.POINTER(trl_solve_info)]),
     "trl_solver_last_error": (C.c_char_p, []),
+    "trl_csr_read_mtx": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(C.POINTER(C.c_int32)),
+                                   C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_double))]),
+    "trl_csr_free_host": (None, [P, P, P]),
 }
 
 _cuda = None
@@ -381,3 +384,25 @@ def solve_csr_device(handle: Handle, A64: DeviceCSRTensors, A32: DeviceCSRTensor
     out = _info_dict(info)
     out.update(evals=evals, resid=resid)
     return out
+
+
+def read_mtx(path: str, threads: int = 0):
+    """Matrix Market coordinate file -> problems.CSRMatrix in full storage, through
+    trl_csr_read_mtx (the reference loader's semantics, examples/sycl/csrevp.hh:26-124)."""
+    from trl_b200 import problems
+
+    L = solver_lib()
+    n, m, nnz = I64(0), I64(0), I64(0)
+    rp, ci, va = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_double)()
+    st = L.trl_csr_read_mtx(os.fsencode(path), threads, C.byref(n), C.byref(m), C.byref(nnz), C.byref(rp), C.byref(ci), C.byref(va))
+    if st != TRL_OK:
+        raise TrlError(st, L.trl_solver_last_error().decode())
+    try:
+        rowptr = np.ctypeslib.as_array(rp, shape=(n.value + 1,)).copy()
+        colind = np.ctypeslib.as_array(ci, shape=(nnz.value,)).copy() if nnz.value else np.zeros(0, np.int32)
+        values = np.ctypeslib.as_array(va, shape=(nnz.value,)).copy() if nnz.value else np.zeros(0)
+    finally:
+        L.trl_csr_free_host(C.cast(rp, P), C.cast(ci, P), C.cast(va, P))
+    if n.value != m.value:
+        raise TrlError(TRL_EINVAL, f"matrix is {n.value} x {m.value}; the eigensolver needs a square one")
+    return problems.CSRMatrix(n.value, rowptr, colind, values)
