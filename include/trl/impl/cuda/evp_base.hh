@@ -16,7 +16,9 @@
 
 #include <cassert>
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
+#include <random>
 #include <memory>
 #include <optional>
 #include <span>
@@ -143,6 +145,54 @@ public:
     gram_seq_ = ctx_->seq();
   }
 
+  /// Partial reorthogonalisation of w against the `count` contiguous blocks starting at V0
+  /// (trl_cuda_project_out_sketch): projects only when the random sketch S of those blocks
+  /// shows a loss of orthogonality above set_partial_threshold() (default 1e-12). S is kept
+  /// here: extended by the blocks added since the last call, rebuilt when the basis changed
+  /// (a restart rotates it into the other multivector, or count went down).
+  void project_out_sketch(BlockView V0, unsigned int count, BlockView w, double eta = 0.70710678118654752)
+  {
+    if (count == 0) return;
+    if (!gram_.get()) gram_ = DeviceBuffer(ctx_, sizeof(double) * blocksize * blocksize);
+    if (!sketch_.get()) sketch_ = DeviceBuffer(ctx_, sizeof(Storage) * N * blocksize);
+    const std::size_t blk = sizeof(Storage) * N * blocksize;
+    constexpr std::size_t bb = blocksize * blocksize;
+    if (count > sketch_coef_blocks_) { // coefficients G_j, entries N(0, 1/bs), one fixed sequence
+      const std::size_t want = std::max<std::size_t>(2 * count, 64);
+      std::vector<double> g(want * bb);
+      std::mt19937_64 rng(0x5eed5eedULL);
+      std::normal_distribution<double> dist(0.0, 1.0 / std::sqrt(static_cast<double>(blocksize)));
+      for (auto& x : g) x = dist(rng);
+      sketch_coef_ = DeviceBuffer(ctx_, sizeof(double) * g.size());
+      ctx_->flush();
+      ctx_->check(trl_cuda_memcpy(ctx_->handle(), sketch_coef_.get(), g.data(), sizeof(double) * g.size(), TRL_H2D), "sketch coefficients");
+      sketch_coef_blocks_ = want;
+    }
+    ctx_->prepare({{V0.data_, blk * count, false}, {w.data_, blk, false}, {w.data_, blk, true}, {sketch_.get(), blk, true}});
+    const auto h = ctx_->handle();
+    const double* coef = static_cast<const double*>(sketch_coef_.get());
+    if (V0.data_ != sketch_v0_ || count < sketch_count_) {
+      ctx_->check(trl_cuda_block_rotate(h, dtype, V0.data_, static_cast<int>(count), coef, 1, 1, sketch_.get(), static_cast<std::int64_t>(N), blocksize), "sketch");
+    }
+    else {
+      for (std::size_t j = sketch_count_; j < count; ++j)
+        ctx_->check(trl_cuda_bv_mult(h, dtype, TRL_MULT_ADD, static_cast<const Storage*>(V0.data_) + j * N * blocksize, coef + j * bb, sketch_.get(),
+                                     static_cast<std::int64_t>(N), blocksize),
+                    "sketch");
+    }
+    sketch_v0_ = V0.data_;
+    sketch_count_ = count;
+    ctx_->check(trl_cuda_project_out_sketch(h, dtype, V0.data_, static_cast<int>(count), w.data_, static_cast<std::int64_t>(N), blocksize, sketch_.get(), partial_threshold_,
+                                            eta, static_cast<double*>(gram_.get())),
+                "project_out_sketch");
+    gram_block_ = w.data_;
+    gram_seq_ = ctx_->seq();
+  }
+
+  /// FP32 storage resolves orthogonality to ~1e-7 only: its threshold is at least 1e-6.
+  void set_partial_threshold(double t) { partial_threshold_ = sizeof(Storage) < 8 ? std::max(t, 1e-6) : t; }
+  double partial_threshold() const { return partial_threshold_; }
+
   Context& context() const { return *ctx_; }
   const std::shared_ptr<Context>& shared_context() const { return ctx_; }
   const double* device_eigenvalues() const { return static_cast<const double*>(evals_dev_.get()); }
@@ -164,6 +214,12 @@ protected:
   int cholqr_passes_ = 2;
   bool full_eigenvectors_ = false;
   std::size_t min_eigenvectors_ = 0;
+  // partial reorthogonalisation: the sketch of the basis and its coefficients
+  double partial_threshold_ = sizeof(Storage) < 8 ? 1e-6 : 1e-12;
+  DeviceBuffer sketch_, sketch_coef_;
+  std::size_t sketch_coef_blocks_ = 0;
+  const Storage* sketch_v0_ = nullptr;
+  std::size_t sketch_count_ = 0;
 };
 
 } // namespace trl::cuda

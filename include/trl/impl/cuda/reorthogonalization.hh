@@ -66,6 +66,27 @@ struct BlockCGS2 {
   }
 };
 
+/// Partial reorthogonalisation: the full projection (with the DGKS second pass where
+/// needed) only at the steps where a random sketch of the basis shows a loss of
+/// orthogonality above the eigenproblem's partial_threshold(); the Lanczos recurrence's own
+/// orthogonalisation against the last two blocks (lanczos.hh:240-253) runs every step.
+struct BlockCGSPartial {
+  double eta = 0.70710678118654752;
+
+  template <typename EVP, typename BMV>
+  void operator()(EVP& evp, BMV& V, unsigned int count, typename BMV::BlockView V_next, typename BMV::BlockMatrix::BlockView tmp) const
+  {
+    if (count == 0) return;
+    if constexpr (requires { evp.project_out_sketch(V.block_view(0), count, V_next, eta); }) {
+      if (evp.euclidean_dot()) {
+        evp.project_out_sketch(V.block_view(0), count, V_next, eta);
+        return;
+      }
+    }
+    detail::per_block_gram_schmidt(evp, V, count, V_next, tmp, 2);
+  }
+};
+
 struct BlockCGSIfNeeded {
   double eta = 0.70710678118654752; // 1/sqrt(2)
 

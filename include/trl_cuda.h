@@ -181,6 +181,15 @@ int trl_cuda_block_update(trl_cuda_handle h, int dtype, void* W, const void* V, 
 enum trl_cgs_mode { TRL_CGS_ONE = 0, TRL_CGS_TWO = 1, TRL_CGS_IFNEEDED = 2 };
 int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, int mode, double eta, double* G);
 
+/* Partial reorthogonalisation (a ReorthogonalizationStrategy beyond the reference's full
+ * ModifiedGS, reorthogonalization.hh:12-22): W is projected against the nblk blocks of V
+ * only when a sketch says it has lost orthogonality to them. S (n x bs, same dtype) is a
+ * random combination of those blocks, S = sum_j V_j G_j with G_j entries N(0, 1/bs), so
+ * that ||S^T W||_F estimates ||V^T W||_F; when ||S^T W||_F > thr ||W||_F pass 1 of
+ * TRL_CGS_IFNEEDED runs (and its DGKS second pass where needed), otherwise W is left as it
+ * is. Decided on the device. G: the Gram matrix of the resulting W. */
+int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, const void* S, double thr, double eta, double* G);
+
 /* trl_cuda_cholqr with the Gram matrix of the first pass supplied (G0 = X^T X on the device,
  * e.g. from trl_cuda_project_out); each further pass forms its Gram matrix while it applies
  * U^{-1}, so CholQR2 reads and writes X twice. G0 == NULL is trl_cuda_cholqr. */

@@ -35,7 +35,7 @@ extern "C" {
 enum trl_mode { TRL_MODE_FP64 = 0, TRL_MODE_FP32 = 1, TRL_MODE_MIXED = 2 };
 /* Reorthogonalisation strategy: the reference's ModifiedGS, or the backend's block classical
  * Gram-Schmidt variants (include/trl/impl/cuda/reorthogonalization.hh). */
-enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEEDED = 2, TRL_REORTH_CGS1 = 3 };
+enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEEDED = 2, TRL_REORTH_CGS1 = 3, TRL_REORTH_PARTIAL = 4 };
 /* FP64 refinement of the mixed mode. */
 enum trl_refine { TRL_REFINE_LANCZOS = 0, TRL_REFINE_CHEBYSHEV = 1 };
 
@@ -60,6 +60,9 @@ typedef struct trl_solve_params {
                                     above ~2e-5, then in FP64 (0: FP64 only) */
   int small_eigen_full;          /* 1: every eigenvector of the projected problem (cuSOLVER
                                     syevd); 0: the kept blocks' only (trl_cuda_small_eigen_partial) */
+  double partial_threshold;      /* TRL_REORTH_PARTIAL: orthogonality loss ||V^T w|| / ||w||
+                                    (sketch estimate) that triggers a projection (0: 1e-12;
+                                    FP32 phases 1e-6 at least) */
 } trl_solve_params;
 
 typedef struct trl_solve_info {

@@ -69,7 +69,7 @@ def cfg1_oracle(oracle):
     return A, X0, r
 
 
-@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS2, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS])
+@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS2, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS, native.TRL_REORTH_PARTIAL])
 @pytest.mark.parametrize("passes", [1, 2])
 def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
     A, X0, ref = cfg1_oracle
@@ -218,7 +218,7 @@ def test_smallest_via_shift(oracle):
     assert np.max(np.abs(out["evals"] - ref["evals"][:8]) / ref["evals"][:8]) < 1e-10
 
 
-@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS1, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_CGS2, native.TRL_REORTH_MGS])
+@pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS1, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_CGS2, native.TRL_REORTH_MGS, native.TRL_REORTH_PARTIAL])
 @pytest.mark.parametrize("batching", [0, 1])
 def test_shifted_small_problem_to_tight_tolerance(reorth, batching):
     """sigma*I - A with a wide spectrum, 12 restart cycles to 1e-12: every block step carries a

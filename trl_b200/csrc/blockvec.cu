@@ -692,6 +692,37 @@ __global__ void k_dgks_flag(const double* __restrict__ G_before, const double* _
   *flag = f;
 }
 
+// flag = ||E||_F^2 > thr2 * trace(G): the sketch S^T W (E) says W's components along the
+// basis exceed thr relative to W's norm (G = W^T W)
+template <int BS>
+__global__ void k_sketch_flag(const double* __restrict__ E, const double* __restrict__ G, double thr2, int* __restrict__ flag)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double e2 = 0.0, tr = 0.0;
+  for (int i = 0; i < BS * BS; ++i) e2 = fma(E[i], E[i], e2);
+  for (int c = 0; c < BS; ++c) tr += G[c * BS + c];
+  *flag = !(e2 <= thr2 * tr); // NaN counts as loss
+}
+
+// flag2 = flag1 && (a column kept less than eta of its norm through pass 1)
+template <int BS>
+__global__ void k_dgks_flag_after(const int* __restrict__ flag1, const double* __restrict__ G_before, const double* __restrict__ G_after, double eta2, int* __restrict__ flag2)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int f = 0;
+  if (*flag1)
+    for (int c = 0; c < BS; ++c) f |= (G_after[c * BS + c] < eta2 * G_before[c * BS + c]);
+  *flag2 = f;
+}
+
+// dst = *f2 ? c : (*f1 ? b : a)  (BS x BS)
+__global__ void k_select_block3(const int* __restrict__ f1, const int* __restrict__ f2, const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
+                                double* __restrict__ dst, int count)
+{
+  const int e = threadIdx.x;
+  if (e < count) dst[e] = *f2 ? c[e] : (*f1 ? b[e] : a[e]);
+}
+
 // dst = *flag ? a : b  (BS x BS)
 __global__ void k_select_block(const int* __restrict__ flag, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ dst, int count)
 {
@@ -1278,6 +1309,58 @@ int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, 
     }
     if (st) return st;
     k_select_block<<<1, 256, 0, h->stream>>>(flag, Gw2, Gw1, G, BB);
+    st = after_launch(h, "select");
+  }));
+  return st;
+}
+
+int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, const void* S, double thr, double eta, double* G)
+{
+  TRL_CHECK_HANDLE(h);
+  if (int st = check_common(h, dtype, n, bs)) return st;
+  if (nblk <= 0 || !G || !(thr >= 0.0)) return set_error(h, TRL_EINVAL, "bad project_out_sketch arguments");
+  const int BB = bs * bs;
+  if (n == 0) return trl_cuda_memset_zero(h, G, sizeof(double) * BB);
+  if (!V || !W || !S) return set_error(h, TRL_EINVAL, "null pointer");
+  // coefficient storage: C1 (nblk blocks) | C2 (nblk blocks) | Gw0 | Gw1 | Gw2 | E | flags
+  double* base = static_cast<double*>(workspace2(h, sizeof(double) * (static_cast<size_t>(2 * nblk + 4) * BB) + 64));
+  if (!base) return TRL_ENOMEM;
+  double* C1 = base;
+  double* C2 = C1 + static_cast<size_t>(nblk) * BB;
+  double* Gw0 = C2 + static_cast<size_t>(nblk) * BB;
+  double* Gw1 = Gw0 + BB;
+  double* Gw2 = Gw1 + BB;
+  double* E = Gw2 + BB;
+  int* flag1 = reinterpret_cast<int*>(E + BB);
+  int* flag2 = flag1 + 1;
+  const size_t es = elt_size(dtype);
+  int st = TRL_OK;
+  TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
+    const T* Vt = static_cast<const T*>(V);
+    const T* St = static_cast<const T*>(S);
+    T* Wt = static_cast<T*>(W);
+    {
+      ProfScope prof(h, PROF_DOT, 3.0 * n * bs * es, 4.0 * n * bs * bs);
+      st = launch_block_dot<T, BS>(h, Wt, 1, Wt, n, Gw0);
+      if (!st) st = launch_block_dot<T, BS>(h, St, 1, Wt, n, E);
+    }
+    if (st) return st;
+    k_sketch_flag<BS><<<1, 32, 0, h->stream>>>(E, Gw0, thr * thr, flag1);
+    if ((st = after_launch(h, "sketch flag"))) return st;
+    // both passes only where flagged (decided on the device; their bytes are not credited
+    // to the profile because the host does not know whether they ran)
+    {
+      ProfScope prof(h, PROF_REORTH2, 0.0);
+      st = launch_block_dot<T, BS>(h, Vt, nblk, Wt, n, C1, flag1);
+      if (!st) st = launch_update_gram<T, BS>(h, Vt, nblk, C1, Wt, n, 1, -1.0, Gw1, flag1);
+      if (st) return st;
+      k_dgks_flag_after<BS><<<1, 32, 0, h->stream>>>(flag1, Gw0, Gw1, eta * eta, flag2);
+      if ((st = after_launch(h, "dgks"))) return st;
+      st = launch_block_dot<T, BS>(h, Vt, nblk, Wt, n, C2, flag2);
+      if (!st) st = launch_update_gram<T, BS>(h, Vt, nblk, C2, Wt, n, 1, -1.0, Gw2, flag2);
+    }
+    if (st) return st;
+    k_select_block3<<<1, 256, 0, h->stream>>>(flag1, flag2, Gw0, Gw1, Gw2, G, BB);
     st = after_launch(h, "select");
   }));
   return st;

@@ -23,7 +23,7 @@ TRL_F64, TRL_F32 = 0, 1
 TRL_H2D, TRL_D2H, TRL_D2D = 0, 1, 2
 TRL_MULT, TRL_MULT_TRANSPOSE, TRL_MULT_ADD, TRL_SUBTRACT, TRL_SUBTRACT_TRANSPOSE = 0, 1, 2, 3, 4
 TRL_MODE_FP64, TRL_MODE_FP32, TRL_MODE_MIXED = 0, 1, 2
-TRL_REORTH_MGS, TRL_REORTH_CGS2, TRL_REORTH_CGS_IFNEEDED, TRL_REORTH_CGS1 = 0, 1, 2, 3
+TRL_REORTH_MGS, TRL_REORTH_CGS2, TRL_REORTH_CGS_IFNEEDED, TRL_REORTH_CGS1, TRL_REORTH_PARTIAL = 0, 1, 2, 3, 4
 TRL_CGS_ONE, TRL_CGS_TWO, TRL_CGS_IFNEEDED = 0, 1, 2
 TRL_REFINE_LANCZOS, TRL_REFINE_CHEBYSHEV = 0, 1
 
@@ -56,6 +56,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_cholqr": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P]),
     "trl_cuda_cholqr_gram": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P, P]),
     "trl_cuda_project_out": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, C.c_int, C.c_double, P]),
+    "trl_cuda_project_out_sketch": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, P, C.c_double, C.c_double, P]),
     "trl_cuda_spmm": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double]),
     "trl_cuda_csr_norm1": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "trl_cuda_spmm3": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double, C.c_double, P]),
@@ -89,7 +90,7 @@ class trl_solve_params(C.Structure):
                 ("tol", C.c_double), ("alpha", C.c_double), ("beta", C.c_double), ("reorth", C.c_int),
                 ("cholqr_passes", C.c_int), ("fp32_tol", C.c_double), ("refine_max_restarts", C.c_uint),
                 ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint), ("refine", C.c_int),
-                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int), ("small_eigen_full", C.c_int)]
+                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int), ("small_eigen_full", C.c_int), ("partial_threshold", C.c_double)]
 
 
 class trl_solve_info(C.Structure):
