@@ -866,6 +866,31 @@ int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, i
   return after_launch(h, "block_dot reduce");
 }
 
+// C = [A, B]^T W (2 blocks of bs x bs) for two blocks anywhere in memory, reading W once:
+// the register kernel's blocks are V and V + vstride.
+template <typename T, int BS>
+int launch_block_dot_two(trl_cuda_context* h, const T* A, const T* B, const T* W, int64_t n, double* C)
+{
+  constexpr int JC = 2, G = 4;
+  constexpr int64_t len = 2 * BS * BS;
+  int64_t target = static_cast<int64_t>(h->num_sms) * 4;
+  int64_t max_chunks = (n + 511) / 512;
+  int64_t chunks = target < max_chunks ? target : max_chunks;
+  if (chunks < 1) chunks = 1;
+  int64_t rows_per_cta = (n + chunks - 1) / chunks;
+  constexpr int step = kWarps * 4 * G;
+  rows_per_cta = (rows_per_cta + step - 1) / step * step;
+  chunks = (n + rows_per_cta - 1) / rows_per_cta;
+  double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
+  if (!partial) return TRL_ENOMEM;
+  const int64_t vstride = B - A; // elements between the two blocks
+  k_block_dot<T, BS, JC, G><<<dim3(1, static_cast<unsigned>(chunks)), kThreads, 0, h->stream>>>(A, vstride, 2, W, n, rows_per_cta, partial, nullptr);
+  int st = after_launch(h, "block_dot");
+  if (st) return st;
+  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, nullptr);
+  return after_launch(h, "block_dot reduce");
+}
+
 template <typename T, int BS, int JC, int S, int TB>
 int launch_block_dot_bulk(trl_cuda_context* h, const T* V, int nblk, const T* W, int64_t n, double* C, const int* cond)
 {
@@ -1322,16 +1347,16 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
   const int BB = bs * bs;
   if (n == 0) return trl_cuda_memset_zero(h, G, sizeof(double) * BB);
   if (!V || !W || !S) return set_error(h, TRL_EINVAL, "null pointer");
-  // coefficient storage: C1 (nblk blocks) | C2 (nblk blocks) | Gw0 | Gw1 | Gw2 | E | flags
+  // coefficient storage: C1 (nblk blocks) | C2 (nblk blocks) | E | Gw0 | Gw1 | Gw2 | flags
   double* base = static_cast<double*>(workspace2(h, sizeof(double) * (static_cast<size_t>(2 * nblk + 4) * BB) + 64));
   if (!base) return TRL_ENOMEM;
   double* C1 = base;
   double* C2 = C1 + static_cast<size_t>(nblk) * BB;
-  double* Gw0 = C2 + static_cast<size_t>(nblk) * BB;
+  double* E = C2 + static_cast<size_t>(nblk) * BB; // [E; Gw0] = [S, W]^T W in one pass
+  double* Gw0 = E + BB;
   double* Gw1 = Gw0 + BB;
   double* Gw2 = Gw1 + BB;
-  double* E = Gw2 + BB;
-  int* flag1 = reinterpret_cast<int*>(E + BB);
+  int* flag1 = reinterpret_cast<int*>(Gw2 + BB);
   int* flag2 = flag1 + 1;
   const size_t es = elt_size(dtype);
   int st = TRL_OK;
@@ -1341,8 +1366,7 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
     T* Wt = static_cast<T*>(W);
     {
       ProfScope prof(h, PROF_DOT, 3.0 * n * bs * es, 4.0 * n * bs * bs);
-      st = launch_block_dot<T, BS>(h, Wt, 1, Wt, n, Gw0);
-      if (!st) st = launch_block_dot<T, BS>(h, St, 1, Wt, n, E);
+      st = launch_block_dot_two<T, BS>(h, St, Wt, Wt, n, E);
     }
     if (st) return st;
     k_sketch_flag<BS><<<1, 32, 0, h->stream>>>(E, Gw0, thr * thr, flag1);
