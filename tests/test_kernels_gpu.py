@@ -249,6 +249,39 @@ def test_cholqr_breakdown_is_reported(cuda_handle):
     cuda_handle.sync()  # the status word is cleared by the report; the context stays usable
 
 
+@pytest.mark.parametrize("bs", [4, 8, 16])
+@pytest.mark.parametrize("dtype", DT)
+def test_project_out_sketch_decides_on_the_device(cuda_handle, bs, dtype):
+    """trl_cuda_project_out_sketch: with a threshold far below the block's orthogonality loss
+    it projects exactly as the if-needed mode; far above, it leaves the block untouched and
+    returns its Gram matrix; the decision follows ||S^T W||_F / ||W||_F."""
+    rng = np.random.default_rng(11 * bs)
+    n, nblk = 2003, 5
+    Q, _ = np.linalg.qr(rng.standard_normal((n, nblk * bs)))
+    V = as_dt(Q.reshape(n, nblk, bs).transpose(1, 0, 2).copy(), dtype)
+    Vf = V.transpose(1, 0, 2).reshape(n, nblk * bs)
+    Gc = rng.standard_normal((nblk, bs, bs)) / np.sqrt(bs)
+    S = as_dt(sum(V[j] @ Gc[j] for j in range(nblk)), dtype)
+    w = as_dt(Vf @ rng.standard_normal((nblk * bs, bs)) * 1e-3 + rng.standard_normal((n, bs)), dtype)
+    eps = 1e-12 if dtype == torch.float64 else 2e-6
+    est = np.linalg.norm(S.T @ w) / np.linalg.norm(w)
+    for thr, projected in ((est / 100, True), (est * 100, False)):
+        Wd = dev(w, dtype)
+        G = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+        cuda_handle.project_out_sketch(dev(V, dtype), Wd, dev(S, dtype), thr, G)
+        got = host(Wd)
+        if projected:
+            Wr = dev(w, dtype)
+            Gr = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+            cuda_handle.project_out(dev(V, dtype), Wr, native.TRL_CGS_IFNEEDED, Gr)
+            close(got, host(Wr), np.abs(w).max(), eps)
+            close(host(G), host(Gr), np.abs(host(Gr)).max(), 1e-12)
+            assert np.abs(Vf.T @ got).max() < 1e3 * eps * np.abs(got).max()
+        else:
+            assert np.array_equal(got, w)
+            close(host(G), w.T @ w, np.abs(w.T @ w).max(), 1e-12 if dtype == torch.float64 else 1e-6)
+
+
 def _random_csr(n, rng, max_deg=40, empty_frac=0.1):
     deg = rng.integers(0, max_deg, size=n)
     deg[rng.random(n) < empty_frac] = 0

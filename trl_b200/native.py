@@ -244,6 +244,10 @@ class Handle:
         nblk, n, bs = V.shape
         self.check(self.lib.trl_cuda_project_out(self.h, _dtype(V), _ptr(V), nblk, _ptr(W), n, bs, mode, eta, _ptr(G)))
 
+    def project_out_sketch(self, V, W, S, thr: float, G, eta: float = 0.7071067811865476):
+        nblk, n, bs = V.shape
+        self.check(self.lib.trl_cuda_project_out_sketch(self.h, _dtype(V), _ptr(V), nblk, _ptr(W), n, bs, _ptr(S), thr, eta, _ptr(G)))
+
     def cholqr_gram(self, X, passes: int, R, G0):
         n, bs = X.shape
         self.check(self.lib.trl_cuda_cholqr_gram(self.h, _dtype(X), _ptr(X), n, bs, passes, _ptr(R), _ptr(G0)))
