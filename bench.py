@@ -364,6 +364,7 @@ def cpu_baseline(A, X0, restarts_gpu: int):
 def profile_case(args):
     """Runs one piece of the workload, without timing output, for profiler captures:
     solve   one FP64 solve capped at --restarts restart cycles (launch lists);
+    mixed   one complete mixed-mode solve (FP32 phase, FP32 and FP64 filter rounds, residuals);
     spmm    the operator apply on the full workload (CSR 113 MB, X and Y 57 MB each);
     dot / update   one multi-block inner product / projection update against --nblk
             basis blocks of the workload (n x 8 FP64 each);
@@ -386,6 +387,12 @@ def profile_case(args):
         X0 = torch.from_numpy(P.initial_block(A.n, bs, seed=CFG["seed"])).cuda()
         mode = native.TRL_MODE_FP32 if args.fp32 else native.TRL_MODE_FP64
         native.solve_csr_device(h, A64, A32, X0, bs=bs, nev=CFG["nev"], ncv=CFG["ncv"], tol=CFG["tol"], mode=mode, max_restarts=args.restarts, want_vectors=0)
+    elif args.case == "mixed":
+        A64 = native.DeviceCSRTensors.from_host(A)
+        A32 = native.DeviceCSRTensors.from_host(A, torch.float32)
+        X0 = torch.from_numpy(P.initial_block(A.n, bs, seed=CFG["seed"])).cuda()
+        native.solve_csr_device(h, A64, A32, X0, bs=bs, nev=CFG["nev"], ncv=CFG["ncv"], tol=CFG["tol"], mode=native.TRL_MODE_MIXED, fp32_tol=args.fp32_tol,
+                                max_restarts=2000, refine_max_restarts=2000, want_vectors=1)
     elif args.case == "spmm":
         Ad = native.DeviceCSRTensors.from_host(A, dt)
         X = torch.randn(A.n, bs, dtype=dt, device="cuda")
@@ -424,7 +431,7 @@ def main():
     ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
     ap.add_argument("--fp32-tol", type=float, default=3e-3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["solve", "spmm", "dot", "update", "project", "rotate"], default=None,
+    ap.add_argument("--case", choices=["solve", "mixed", "spmm", "dot", "update", "project", "rotate"], default=None,
                     help="profiling driver: run one piece of the workload and exit (see profile_case)")
     ap.add_argument("--restarts", type=int, default=3)
     ap.add_argument("--nblk", type=int, default=24)
