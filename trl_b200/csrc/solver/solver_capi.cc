@@ -357,7 +357,8 @@ private:
     int nconv = 0;
     double* zero = static_cast<double*>(small_.get()) + 2 * bs * bs;
     ctx_->check(trl_cuda_mb_zero(h_, zero, bs), "refine Rayleigh-Ritz");
-    ctx_->check(trl_cuda_small_eigen(h_, T, static_cast<int>(kr_), bs, zero, 0, 1.0, static_cast<double*>(ev_.get()), static_cast<double*>(Z_.get()), theta.data(), &nconv),
+    ctx_->check(trl_cuda_small_eigen_partial(h_, T, static_cast<int>(kr_), bs, zero, 0, 1.0, static_cast<int>(N), static_cast<double*>(ev_.get()), static_cast<double*>(Z_.get()),
+                                             theta.data(), &nconv),
                 "refine Rayleigh-Ritz");
     const double* Z = static_cast<const double*>(Z_.get());
     ctx_->check(trl_cuda_block_rotate(h_, TRL_F64, X, static_cast<int>(kr_), Z, static_cast<int>(kr_), static_cast<int>(kr_), out, n_, bs), "refine Rayleigh-Ritz");
