@@ -7,6 +7,10 @@
 // Layout: a block vector is n x BS row-major; block j of a multivector at base + j*n*BS.
 #include "common.cuh"
 
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+
 namespace {
 
 constexpr int kThreads = 256; // 8 warps per CTA for every kernel in this file
@@ -1386,6 +1390,19 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
     if (st) return st;
     k_select_block3<<<1, 256, 0, h->stream>>>(flag1, flag2, Gw0, Gw1, Gw2, G, BB);
     st = after_launch(h, "select");
+    // TRL_PARTIAL_TRACE: one stderr line per call (synchronises; diagnostics only)
+    static const bool trace = std::getenv("TRL_PARTIAL_TRACE") != nullptr;
+    if (!st && trace) {
+      double eg[2 * 256];
+      int fl[2];
+      cudaMemcpyAsync(eg, E, sizeof(double) * 2 * BB, cudaMemcpyDeviceToHost, h->stream);
+      cudaMemcpyAsync(fl, flag1, sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream);
+      cudaStreamSynchronize(h->stream);
+      double e2 = 0.0, tr = 0.0;
+      for (int i = 0; i < BB; ++i) e2 += eg[i] * eg[i];
+      for (int c = 0; c < bs; ++c) tr += eg[BB + c * bs + c];
+      std::fprintf(stderr, "partial nblk %d loss %.3e projected %d second %d\n", nblk, std::sqrt(e2 / tr), fl[0], fl[1]);
+    }
   }));
   return st;
 }
