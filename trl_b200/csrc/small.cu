@@ -864,8 +864,14 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   if (!valid_bs(bs) || nblk <= 0 || !T || !beta || !evals || !evecs || !host_evals || !host_nconv) return set_error(h, TRL_EINVAL, "bad small_eigen arguments");
   const int N = nblk * bs;
   if (kvec < 0 || kvec > N) return set_error(h, TRL_EINVAL, "kvec %d outside [0, %d]", kvec, N);
-  static int cluster_ok = -1; // whether a kTriC-CTA cluster with the shared memory of N = kTriMaxN can be resident
-  if (cluster_ok < 0) {
+  // per device (function attributes are set for the current device): whether a kTriC-CTA
+  // cluster with the shared memory of N = kTriMaxN can be resident
+  static int cluster_ok_dev[64];
+  static bool cluster_checked[64];
+  if (h->device < 0 || h->device >= 64) return set_error(h, TRL_EINVAL, "device index %d", h->device);
+  int& cluster_ok = cluster_ok_dev[h->device];
+  if (!cluster_checked[h->device]) {
+    cluster_checked[h->device] = true;
     cluster_ok = 0;
     const size_t smem = tridiag_smem(kTriMaxN);
     if (cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) == cudaSuccess &&
