@@ -900,9 +900,13 @@ int launch_block_dot_bulk(trl_cuda_context* h, const T* V, int nblk, const T* W,
 {
   constexpr int R = BulkTile<T, BS, TB>::R;
   constexpr size_t smem = static_cast<size_t>(S) * (JC + 1) * BulkTile<T, BS, TB>::ELEMS * sizeof(T) + 2 * S * sizeof(uint64_t);
-  static int resident = 0; // CTAs per SM at this shared-memory size (queried once)
+  // the shared-memory attribute belongs to the current device: set it on every call
+  if (cudaFuncSetAttribute(k_block_dot_bulk<T, BS, JC, S, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(h, TRL_ECUDA, "block dot: %zu bytes of shared memory refused", smem);
+  }
+  static int resident = 0; // CTAs per SM at this shared-memory size (queried once; same on every B200)
   if (resident == 0) {
-    cudaFuncSetAttribute(k_block_dot_bulk<T, BS, JC, S, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_block_dot_bulk<T, BS, JC, S, TB>, kThreads, smem) != cudaSuccess || resident < 1) resident = 1;
     cudaGetLastError();
   }
