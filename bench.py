@@ -362,9 +362,11 @@ def cpu_baseline(A, X0, restarts_gpu: int):
 
 
 def profile_case(args):
-    """Runs one piece of the workload, without timing output, for profiler captures:
+    """Runs one piece of the workload for profiler captures (without timing output, except
+    spmm-zipf, which prints one JSON line of throughput per block size and precision):
     solve   one FP64 solve capped at --restarts restart cycles (launch lists);
     mixed   one complete mixed-mode solve (FP32 phase, FP32 and FP64 filter rounds, residuals);
+    spmm-zipf  SpMM throughput on the 4M-row Zipf operator, block sizes 4/8/16, FP64 and FP32;
     spmm    the operator apply on the full workload (CSR 113 MB, X and Y 57 MB each);
     dot / update   one multi-block inner product / projection update against --nblk
             basis blocks of the workload (n x 8 FP64 each);
@@ -393,6 +395,36 @@ def profile_case(args):
         X0 = torch.from_numpy(P.initial_block(A.n, bs, seed=CFG["seed"])).cuda()
         native.solve_csr_device(h, A64, A32, X0, bs=bs, nev=CFG["nev"], ncv=CFG["ncv"], tol=CFG["tol"], mode=native.TRL_MODE_MIXED, fp32_tol=args.fp32_tol,
                                 max_restarts=2000, refine_max_restarts=2000, want_vectors=1)
+    elif args.case == "spmm-zipf":
+        # the bandwidth-stress operator: n = 4,194,304, Zipf(1.5) out-degrees capped at 512,
+        # mirrored (about 145M entries); SpMM throughput per block size and precision, each
+        # timed launch behind an L2 flush
+        hbm, _, src = peaks()
+        Z = P.zipf_symmetric(4_194_304, cap=512, seed=42)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        for dt, name in ((torch.float64, "f64"), (torch.float32, "f32")):
+            Zd = native.DeviceCSRTensors.from_host(Z, dt)
+            es = 8 if dt == torch.float64 else 4
+            for b in (4, 8, 16):
+                X = torch.randn(Z.n, b, dtype=dt, device="cuda")
+                Y = torch.empty_like(X)
+                for _ in range(3):
+                    h.spmm(Zd, X, Y)
+                times = []
+                for _ in range(max(args.reps, 5)):
+                    flush.fill_(1)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    h.spmm(Zd, X, Y)
+                    e1.record()
+                    torch.cuda.synchronize()
+                    times.append(e0.elapsed_time(e1) / 1e3)
+                t = statistics.median(times)
+                nbytes = Z.nnz * (es + 4) + 4 * (Z.n + 1) + 2 * Z.n * b * es
+                print(json.dumps({"case": "spmm-zipf", "dtype": name, "bs": b, "n": Z.n, "nnz": int(Z.nnz), "us": t * 1e6, "gbs": nbytes / t / 1e9,
+                                  "frac_of_hbm": nbytes / t / 1e9 / hbm, "peak_source": src}), flush=True)
+                del X, Y
+            del Zd
     elif args.case == "spmm":
         Ad = native.DeviceCSRTensors.from_host(A, dt)
         X = torch.randn(A.n, bs, dtype=dt, device="cuda")
@@ -431,7 +463,7 @@ def main():
     ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
     ap.add_argument("--fp32-tol", type=float, default=3e-3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["solve", "mixed", "spmm", "dot", "update", "project", "rotate"], default=None,
+    ap.add_argument("--case", choices=["solve", "mixed", "spmm", "spmm-zipf", "dot", "update", "project", "rotate"], default=None,
                     help="profiling driver: run one piece of the workload and exit (see profile_case)")
     ap.add_argument("--restarts", type=int, default=3)
     ap.add_argument("--nblk", type=int, default=24)
