@@ -506,6 +506,56 @@ def test_spmm_on_elasticity_and_zipf_patterns(cuda_handle, oracle, bs, dtype):
         close(host(Yd), ref, mag.max(), 1e-12 if dtype == torch.float64 else 2e-6)
 
 
+def _long_row_csr(rng, n=4099):
+    """Short rows (0-5 entries) around long ones placed where the warp-wide sweep of long
+    rows has its edge cases: every 37th row 33-699 entries (longer than a stage chunk), the
+    last row of a 4/8/16/32-row warp iteration, an iteration of mixed long rows (64-71),
+    rows of exactly 32 (not swept) and 33 entries alone in an iteration, and a long last
+    row with n a multiple of no iteration width."""
+    deg = rng.integers(0, 6, size=n)
+    every = np.arange(n) % 37 == 5
+    deg[every] = rng.integers(33, 700, size=every.sum())
+    deg[[7, 15, 31, 63]] = 400
+    deg[64:72] = [33, 40, 50, 300, 500, 33, 64, 129]
+    deg[128:136] = [32, 0, 0, 0, 0, 0, 0, 0]
+    deg[136:144] = [33, 0, 0, 0, 0, 0, 0, 0]
+    deg[n - 1] = 600
+    rows = np.repeat(np.arange(n), deg)
+    cols = np.concatenate([rng.choice(n, size=d, replace=False) for d in deg])
+    return P._from_coo(n, rows, cols, rng.standard_normal(rows.size))
+
+
+@pytest.mark.parametrize("bs", BS)
+@pytest.mark.parametrize("dtype", DT)
+def test_spmm_long_rows_swept_by_the_warp(cuda_handle, oracle, bs, dtype):
+    """Rows much longer than their warp iteration's mean are summed by all row groups of
+    the warp; the one-block entry points (plain and three-term) and the multi-block one
+    (which walks them per row) all match the oracle."""
+    rng = np.random.default_rng(23)
+    A = _long_row_csr(rng)
+    vals = A.values.astype(np.float32).astype(np.float64) if dtype == torch.float32 else A.values
+    Ah = P.CSRMatrix(A.n, A.rowptr, A.colind, vals)
+    Ad = native.DeviceCSRTensors.from_host(Ah, dtype)
+    X = as_dt(rng.standard_normal((2, A.n, bs)), dtype)
+    W = as_dt(rng.standard_normal((A.n, bs)), dtype)
+    rows = A.row_indices()
+    mag = np.zeros(A.n)
+    np.add.at(mag, rows, np.abs(vals) * np.abs(X).max(axis=(0, 2))[A.colind])
+    tol = 1e-12 if dtype == torch.float64 else 2e-6
+    Yd = torch.full((A.n, bs), float("nan"), dtype=dtype, device="cuda")
+    cuda_handle.spmm(Ad, dev(X[0], dtype), Yd)
+    close(host(Yd), oracle.spmm(Ah, X[0]), mag.max(), tol)
+    alpha, beta, gamma = -0.5, 2.0, 0.25
+    ref = np.stack([oracle.spmm(Ah, X[j], alpha, beta) for j in range(2)])
+    scale = abs(alpha) * mag.max() + abs(beta) * np.abs(X).max() + abs(gamma) * np.abs(W).max()
+    Yd = dev(W, dtype)
+    cuda_handle.spmm3(Ad, dev(X[0], dtype), Yd, alpha, beta, gamma, Yd)
+    close(host(Yd), ref[0] + gamma * W, scale, tol)
+    Yd = torch.full((2, A.n, bs), float("nan"), dtype=dtype, device="cuda")
+    cuda_handle.spmm_blocks(Ad, dev(X, dtype), Yd, alpha, beta, 0.0, None)
+    close(host(Yd), ref, scale, tol)
+
+
 @pytest.mark.parametrize("bs", BS)
 @pytest.mark.parametrize("dtype", DT)
 @pytest.mark.parametrize("nb", [1, 3, 5])
@@ -536,13 +586,18 @@ def test_spmm_blocks_three_term(cuda_handle, oracle, bs, dtype, nb):
         Yd = dev(W, dtype)
         cuda_handle.spmm_blocks(Ad, Xd, Yd, alpha, beta, gamma, Yd)
         close(host(Yd), ref + gamma * W, scale, tol)
-        # no W: matches the one-block entry point block by block
+        # no W: matches the one-block entry point block by block - bit for bit where no row
+        # is swept by the whole warp (the stencil); the multi-block walk takes Zipf's long
+        # rows per row, in another summation order
         Yd = torch.full((nb, A.n, bs), float("nan"), dtype=dtype, device="cuda")
         cuda_handle.spmm_blocks(Ad, Xd, Yd, alpha, beta, 0.0, None)
         for j in range(nb):
             Y1 = torch.empty((A.n, bs), dtype=dtype, device="cuda")
             cuda_handle.spmm3(Ad, Xd[j], Y1, alpha, beta, 0.0, None)
-            assert torch.equal(Yd[j], Y1)
+            if np.diff(A.rowptr).max() > 32:
+                close(host(Yd[j]), host(Y1), scale, tol)
+            else:
+                assert torch.equal(Yd[j], Y1)
         close(host(Yd), ref, scale, tol)
 
 

@@ -81,6 +81,12 @@ struct SpmmShape {
   static constexpr int MINB = sizeof(T) == 8 ? 6 : 4;    // CTAs per SM the registers must allow
 };
 
+// A row of a warp iteration is swept by all the warp's row groups together when it holds
+// more than kLongRow entries and more than twice the iteration's mean row length: the
+// per-row walk keeps every group busy for the longest row's length, which on a Zipf row-length
+// pattern (median 21, p99 326) leaves 70% of the lane slots idle.
+constexpr int kLongRow = 32;
+
 // The CSR stream is read once: load it without allocating in L1, which keeps L1 for the
 // X rows that neighbouring rows gather again.
 __device__ __forceinline__ int ld_stream(const int32_t* p)
@@ -108,8 +114,12 @@ __device__ __forceinline__ float ld_stream(const float* p)
 //  2. the rows' (col, val) pairs - one contiguous CSR range - are staged in shared memory
 //     with coalesced warp-wide loads, CH pairs at a time;
 //  3. each group walks its row's pairs in the stage and issues UG independent X gathers
-//     (16 bytes per lane) before the FMAs that consume them.
-//  With MB (several blocks), a range that fits one stage is staged once for all blocks.
+//     (16 bytes per lane) before the FMAs that consume them;
+//  4. long rows (kLongRow) are left out of step 3 and swept afterwards, one at a time, by
+//     all groups (group g takes every RPW-th pair from g), then summed over the groups
+//     with butterfly shuffles. Chunks that hold only long-row pairs are not staged in step 2.
+//  With MB (several blocks), a range that fits one stage is staged once for all blocks and
+//  walked per row.
 template <typename T, int BS, bool MB>
 __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
                                                                          const T* __restrict__ vals, const T* __restrict__ X, T* Y, T alpha, T beta, T gamma,
@@ -118,6 +128,9 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
   using S = SpmmShape<T, BS>;
   constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH, PF = S::PF;
   constexpr int WPC = kThreads / 32;
+  // The multi-block walk and FP64 with one column per lane have no registers left for the
+  // long-row sweep under the 6-CTA bound (ptxas spills them); they walk every row per row.
+  constexpr bool COOP = !MB && !(sizeof(T) == 8 && BS == 1);
   __shared__ int s_col[WPC][CH];
   __shared__ T s_val[WPC][CH];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -147,26 +160,35 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
     // (X, Y, W hold nb blocks bstride elements apart); longer ranges are staged chunk by
     // chunk for each block.
     const bool one_chunk = MB && (e - s) <= CH; // uniform over the warp
-    auto stage = [&](int cs) {
+    // bit r: row r of this iteration is swept by the whole warp (lane r < RPW tests row r)
+    unsigned longs = 0;
+    if (COOP && !one_chunk) {
+      const int nx = __shfl_sync(0xffffffffu, rp0, (lane + 1) & 31);
+      const int len = (lane + 1 == RPW ? rpe0 : nx) - rp0;
+      longs = __ballot_sync(0xffffffffu, lane < RPW && len > kLongRow && static_cast<int64_t>(len) * RPW > 2 * static_cast<int64_t>(e - s));
+    }
+    const int kw = ((longs >> grp) & 1u) ? kb : ke; // end of this group's per-row walk
+    auto stage = [&](int cs, int end) {
 #pragma unroll
       for (int q = 0; q < PF; ++q) {
         const int p = cs + q * 32 + lane;
-        if (p < e) {
+        if (p < end) {
           s_col[w][q * 32 + lane] = ld_stream(colind + p);
           s_val[w][q * 32 + lane] = ld_stream(vals + p);
         }
       }
       __syncwarp();
     };
-    if (one_chunk) stage(s);
+    if (one_chunk) stage(s, e);
     for (int b = 0; b < (MB ? nb : 1); ++b) {
       const T* Xb = X + static_cast<int64_t>(b) * bstride;
       T acc[VEC];
 #pragma unroll
       for (int i = 0; i < VEC; ++i) acc[i] = T(0);
       for (int cs = s; cs < e; cs += CH) {
-        if (!one_chunk) stage(cs);
-        const int lo = max(kb, cs) - cs, hi = min(ke, cs + CH) - cs;
+        const int lo = max(kb, cs) - cs, hi = min(kw, cs + CH) - cs;
+        if (longs != 0 && !__any_sync(0xffffffffu, lo < hi)) continue; // only long-row pairs
+        if (!one_chunk) stage(cs, e);
         for (int t = lo; t < hi; t += UG) {
           T x[UG][VEC];
           T wv[UG];
@@ -188,6 +210,51 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
             for (int i = 0; i < VEC; ++i) acc[i] = fma(wv[u], x[u][i], acc[i]);
         }
         if (!one_chunk) __syncwarp(); // the stage is rewritten by the next chunk
+      }
+
+      for (unsigned m = longs; m != 0; m &= m - 1) { // warp-uniform
+        const int r = __ffs(m) - 1;
+        const int rb = __shfl_sync(0xffffffffu, rp0, r);
+        const int rn = __shfl_sync(0xffffffffu, rp0, (r + 1) & 31);
+        const int re = (r + 1 == RPW) ? rpe0 : rn;
+        T lacc[VEC];
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) lacc[i] = T(0);
+        for (int cs = rb; cs < re; cs += CH) {
+          stage(cs, re);
+          const int cnt = min(re - cs, CH);
+          for (int t = grp; t < cnt; t += RPW * UG) {
+            T x[UG][VEC];
+            T wv[UG];
+#pragma unroll
+            for (int u = 0; u < UG; ++u) {
+              const int tu = t + u * RPW;
+              if (tu < cnt) {
+                wv[u] = s_val[w][tu];
+                load_vec<T, VEC>(Xb + static_cast<int64_t>(s_col[w][tu]) * BS + sub * VEC, x[u]);
+              }
+              else {
+                wv[u] = T(0);
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) x[u][i] = T(0);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < UG; ++u)
+#pragma unroll
+              for (int i = 0; i < VEC; ++i) lacc[i] = fma(wv[u], x[u][i], lacc[i]);
+          }
+          __syncwarp(); // the stage is rewritten by the next chunk
+        }
+        // lane = grp * LPR + sub: sum over the group bits
+#pragma unroll
+        for (int off = LPR; off < 32; off <<= 1)
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) lacc[i] += __shfl_xor_sync(0xffffffffu, lacc[i], off);
+        if (grp == r) {
+#pragma unroll
+          for (int i = 0; i < VEC; ++i) acc[i] = lacc[i];
+        }
       }
 
       const int64_t row = rbase + grp;
