@@ -160,14 +160,13 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
     // (X, Y, W hold nb blocks bstride elements apart); longer ranges are staged chunk by
     // chunk for each block.
     const bool one_chunk = MB && (e - s) <= CH; // uniform over the warp
-    // bit r: row r of this iteration is swept by the whole warp (lane r < RPW tests row r)
-    unsigned longs = 0;
-    if (COOP && !one_chunk) {
-      const int nx = __shfl_sync(0xffffffffu, rp0, (lane + 1) & 31);
-      const int len = (lane + 1 == RPW ? rpe0 : nx) - rp0;
-      longs = __ballot_sync(0xffffffffu, lane < RPW && len > kLongRow && static_cast<int64_t>(len) * RPW > 2 * static_cast<int64_t>(e - s));
-    }
-    const int kw = ((longs >> grp) & 1u) ? kb : ke; // end of this group's per-row walk
+    // Each group tests its own row (len * RPW > 2 (e - s), without overflow); bit g * LPR of
+    // `longs` marks row g. No shuffle: the walk is bound by the shared-memory/L1 pipe, where
+    // one more shuffle per iteration cost the stencil 4%.
+    const int len = ke - kb;
+    const bool mine_long = COOP && !one_chunk && len > kLongRow && static_cast<unsigned>(len) > static_cast<unsigned>(e - s) / (RPW / 2);
+    const unsigned longs = COOP ? __ballot_sync(0xffffffffu, mine_long && sub == 0) : 0u;
+    const int kw = mine_long ? kb : ke; // end of this group's per-row walk
     auto stage = [&](int cs, int end) {
 #pragma unroll
       for (int q = 0; q < PF; ++q) {
@@ -213,10 +212,9 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
       }
 
       for (unsigned m = longs; m != 0; m &= m - 1) { // warp-uniform
-        const int r = __ffs(m) - 1;
-        const int rb = __shfl_sync(0xffffffffu, rp0, r);
-        const int rn = __shfl_sync(0xffffffffu, rp0, (r + 1) & 31);
-        const int re = (r + 1 == RPW) ? rpe0 : rn;
+        const int r = (__ffs(m) - 1) / LPR; // the row, and the group that writes it
+        const int rb = __shfl_sync(0xffffffffu, kb, r * LPR);
+        const int re = __shfl_sync(0xffffffffu, ke, r * LPR);
         T lacc[VEC];
 #pragma unroll
         for (int i = 0; i < VEC; ++i) lacc[i] = T(0);
