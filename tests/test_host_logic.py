@@ -142,3 +142,19 @@ def test_bench_max_over_ranks_gloo():
         assert p.exitcode == 0
     vals = sorted(q.get(timeout=10) for _ in range(2))
     assert vals == [(0, 3.0), (1, 3.0)]
+
+
+def test_solve_csr_host_rejects_bad_eigenvector_buffers():
+    """The caller's eigenvector buffer is checked before anything reaches the library."""
+    import numpy as np
+
+    from trl_b200 import native
+    from trl_b200 import problems as P
+
+    A = P.laplace2d(8)
+    X0 = np.zeros((A.n, 4))
+    ro = np.zeros((A.n, 10))
+    ro.flags.writeable = False
+    for bad in (np.zeros((A.n, 9)), np.zeros((A.n, 10), dtype=np.float32), np.zeros((10, A.n)).T, ro, [[0.0] * 10] * A.n):
+        with pytest.raises(ValueError):
+            native.solve_csr_host(A, X0, evecs_out=bad, bs=4, nev=10, ncv=160)

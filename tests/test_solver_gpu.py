@@ -86,6 +86,21 @@ def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
     assert abs(out["restarts"] - ref["iterations"]) <= max(3, ref["iterations"] // 5)
 
 
+def test_eigenvectors_into_the_callers_buffer(cfg1_oracle):
+    """evecs_out (here page-locked, as a repeated caller keeps it) receives exactly what the
+    allocating call returns, and is returned itself."""
+    import torch
+
+    A, X0, ref = cfg1_oracle
+    kw = dict(bs=4, nev=10, ncv=160, tol=1e-8)
+    buf = torch.full((A.n, 10), float("nan"), dtype=torch.float64).pin_memory().numpy()
+    mine = native.solve_csr_host(A, X0, evecs_out=buf, **kw)
+    fresh = native.solve_csr_host(A, X0, **kw)
+    assert mine["evecs"] is buf
+    assert np.array_equal(buf, fresh["evecs"])
+    assert np.array_equal(mine["evals"], fresh["evals"])
+
+
 @pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS])
 def test_fused_and_call_by_call_execution_agree(cfg1_oracle, reorth):
     """batching = 1 fuses the three-term step's product/subtract pairs (deferring the

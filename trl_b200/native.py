@@ -353,16 +353,26 @@ def _info_dict(info: trl_solve_info) -> dict:
     return {name: getattr(info, name) for name, _ in trl_solve_info._fields_}
 
 
-def solve_csr_host(A, X0: np.ndarray, device: int = 0, vectors: bool = True, **params) -> dict:
-    """Host-in/host-out solve through trl_solve_csr_host."""
+def solve_csr_host(A, X0: np.ndarray, device: int = 0, vectors: bool = True, evecs_out: np.ndarray | None = None, **params) -> dict:
+    """Host-in/host-out solve through trl_solve_csr_host.
+
+    evecs_out: optional (n, nev) C-contiguous float64 array that receives the eigenvectors
+    (implies vectors=True). A caller that solves repeatedly passes one page-locked buffer
+    here: the download of a freshly allocated array runs at pageable-copy speed and faults
+    in every page (about 50 ms for 226 MB)."""
     p = default_params(**params)
     n = A.n
+    if evecs_out is not None:
+        if not isinstance(evecs_out, np.ndarray) or evecs_out.dtype != np.float64 or evecs_out.shape != (n, p.nev) or not evecs_out.flags.c_contiguous:
+            raise ValueError(f"evecs_out must be a C-contiguous float64 array of shape ({n}, {p.nev})")
+        if not evecs_out.flags.writeable:
+            raise ValueError("evecs_out must be writeable")
     X0 = np.ascontiguousarray(X0, dtype=np.float64).reshape(n, p.bs)
     rp = np.ascontiguousarray(A.rowptr, dtype=np.int32)
     ci = np.ascontiguousarray(A.colind, dtype=np.int32)
     va = np.ascontiguousarray(A.values, dtype=np.float64)
     evals = np.zeros(p.nev)
-    evecs = np.zeros((n, p.nev)) if vectors else None
+    evecs = evecs_out if evecs_out is not None else (np.zeros((n, p.nev)) if vectors else None)
     resid = np.zeros(p.nev)
     info = trl_solve_info()
     L = solver_lib()
