@@ -149,12 +149,20 @@ public:
   /// (trl_cuda_project_out_sketch): projects only when the random sketch S of those blocks
   /// shows a loss of orthogonality above set_partial_threshold() (default 1e-12). S is kept
   /// here: extended by the blocks added since the last call, rebuilt when the basis changed
-  /// (a restart rotates it into the other multivector, or count went down).
+  /// (a restart rotates it into the other multivector, or count went down). With
+  /// set_partial_pairs (the default) a step whose test fired also projects the next step:
+  /// projected alone, a step leaves the loss of its unprojected predecessor to return two
+  /// steps later through the recurrence's B term.
   void project_out_sketch(BlockView V0, unsigned int count, BlockView w, double eta = 0.70710678118654752)
   {
     if (count == 0) return;
     if (!gram_.get()) gram_ = DeviceBuffer(ctx_, sizeof(double) * blocksize * blocksize);
     if (!sketch_.get()) sketch_ = DeviceBuffer(ctx_, sizeof(Storage) * N * blocksize);
+    if (!sketch_pair_.get()) {
+      sketch_pair_ = DeviceBuffer(ctx_, sizeof(int));
+      ctx_->flush();
+      ctx_->check(trl_cuda_memset_zero(ctx_->handle(), sketch_pair_.get(), sizeof(int)), "sketch pair state");
+    }
     const std::size_t blk = sizeof(Storage) * N * blocksize;
     constexpr std::size_t bb = blocksize * blocksize;
     if (count > sketch_coef_blocks_) { // coefficients G_j, entries N(0, 1/bs), one fixed sequence
@@ -183,7 +191,7 @@ public:
     sketch_v0_ = V0.data_;
     sketch_count_ = count;
     ctx_->check(trl_cuda_project_out_sketch(h, dtype, V0.data_, static_cast<int>(count), w.data_, static_cast<std::int64_t>(N), blocksize, sketch_.get(), partial_threshold_,
-                                            eta, static_cast<double*>(gram_.get())),
+                                            eta, static_cast<double*>(gram_.get()), partial_pairs_ ? static_cast<int*>(sketch_pair_.get()) : nullptr),
                 "project_out_sketch");
     gram_block_ = w.data_;
     gram_seq_ = ctx_->seq();
@@ -192,6 +200,8 @@ public:
   /// FP32 storage resolves orthogonality to ~1e-7 only: its threshold is at least 1e-6.
   void set_partial_threshold(double t) { partial_threshold_ = sizeof(Storage) < 8 ? std::max(t, 1e-6) : t; }
   double partial_threshold() const { return partial_threshold_; }
+  void set_partial_pairs(bool on) { partial_pairs_ = on; }
+  bool partial_pairs() const { return partial_pairs_; }
 
   Context& context() const { return *ctx_; }
   const std::shared_ptr<Context>& shared_context() const { return ctx_; }
@@ -216,7 +226,8 @@ protected:
   std::size_t min_eigenvectors_ = 0;
   // partial reorthogonalisation: the sketch of the basis and its coefficients
   double partial_threshold_ = sizeof(Storage) < 8 ? 1e-6 : 1e-12;
-  DeviceBuffer sketch_, sketch_coef_;
+  bool partial_pairs_ = true;
+  DeviceBuffer sketch_, sketch_coef_, sketch_pair_;
   std::size_t sketch_coef_blocks_ = 0;
   const Storage* sketch_v0_ = nullptr;
   std::size_t sketch_count_ = 0;

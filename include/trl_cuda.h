@@ -187,8 +187,14 @@ int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, 
  * random combination of those blocks, S = sum_j V_j G_j with G_j entries N(0, 1/bs), so
  * that ||S^T W||_F estimates ||V^T W||_F; when ||S^T W||_F > thr ||W||_F pass 1 of
  * TRL_CGS_IFNEEDED runs (and its DGKS second pass where needed), otherwise W is left as it
- * is. Decided on the device. G: the Gram matrix of the resulting W. */
-int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, const void* S, double thr, double eta, double* G);
+ * is. Decided on the device. G: the Gram matrix of the resulting W.
+ * pair_state (device int, zero-initialised, kept by the caller across the steps of one
+ * recurrence; NULL: off): a step whose sketch test fired also projects the next step. In a
+ * three-term recurrence W_{i+1} inherits the loss of V_{i-1} through its B term, so
+ * projecting one step alone leaves the loss to return two steps later (Simon's partial
+ * reorthogonalisation projects pairs for the same reason). */
+int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, const void* S, double thr, double eta, double* G,
+                                int* pair_state);
 
 /* trl_cuda_cholqr with the Gram matrix of the first pass supplied (G0 = X^T X on the device,
  * e.g. from trl_cuda_project_out); each further pass forms its Gram matrix while it applies

@@ -63,6 +63,8 @@ typedef struct trl_solve_params {
   double partial_threshold;      /* TRL_REORTH_PARTIAL: orthogonality loss ||V^T w|| / ||w||
                                     (sketch estimate) that triggers a projection (0: 1e-12;
                                     FP32 phases 1e-6 at least) */
+  int partial_pairs;             /* TRL_REORTH_PARTIAL: a step whose sketch test fired also
+                                    projects the next step (1, default; 0: that step only) */
 } trl_solve_params;
 
 typedef struct trl_solve_info {

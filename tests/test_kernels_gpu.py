@@ -282,6 +282,52 @@ def test_project_out_sketch_decides_on_the_device(cuda_handle, bs, dtype):
             close(host(G), w.T @ w, np.abs(w.T @ w).max(), 1e-12 if dtype == torch.float64 else 1e-6)
 
 
+@pytest.mark.parametrize("dtype", DT)
+def test_project_out_sketch_pairs(cuda_handle, dtype):
+    """With a pair state, a step whose sketch test fired also projects the next step (one
+    step only: a forced projection forces nothing). 'loud' blocks exceed the threshold 100x;
+    'quiet' ones carry a component along V 10x below it, which a projection removes and
+    which otherwise stays bit for bit."""
+    bs, n, nblk = 8, 2003, 5
+    rng = np.random.default_rng(5)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, nblk * bs)))
+    V = as_dt(Q.reshape(n, nblk, bs).transpose(1, 0, 2).copy(), dtype)
+    Vf = V.transpose(1, 0, 2).reshape(n, nblk * bs)
+    Gc = rng.standard_normal((nblk, bs, bs)) / np.sqrt(bs)
+    S = as_dt(sum(V[j] @ Gc[j] for j in range(nblk)), dtype)
+
+    def block(scale):
+        r = rng.standard_normal((n, bs))
+        r -= Vf @ (Vf.T @ r)
+        return as_dt(r + scale * (Vf @ rng.standard_normal((nblk * bs, bs))), dtype)
+
+    def est(x):
+        return np.linalg.norm(S.T @ x) / np.linalg.norm(x)
+
+    loud = block(0.3)
+    thr = est(loud) / 100
+    quiet = block(0.3 / 1000)
+    assert est(quiet) < thr / 3
+    seq = [quiet, loud, quiet, quiet, loud, loud, quiet, quiet]
+    eps = 1e-12 if dtype == torch.float64 else 2e-6
+    for pairs, expect in ((True, [0, 1, 1, 0, 1, 1, 1, 0]), (False, [0, 1, 0, 0, 1, 1, 0, 0])):
+        state = torch.zeros(1, dtype=torch.int32, device="cuda") if pairs else None
+        got = []
+        for x in seq:
+            Wd = dev(x, dtype)
+            G = torch.zeros((bs, bs), dtype=torch.float64, device="cuda")
+            cuda_handle.project_out_sketch(dev(V, dtype), Wd, dev(S, dtype), thr, G, pair_state=state)
+            out = host(Wd)
+            if np.array_equal(out, x):
+                got.append(0)
+            else:
+                assert np.abs(Vf.T @ out).max() < 1e3 * eps * np.abs(out).max()
+                got.append(1)
+        assert got == expect, (pairs, got)
+        if pairs:
+            assert int(state.item()) == 0  # the last step's test did not fire
+
+
 def _random_csr(n, rng, max_deg=40, empty_frac=0.1):
     deg = rng.integers(0, max_deg, size=n)
     deg[rng.random(n) < empty_frac] = 0

@@ -86,6 +86,20 @@ def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
     assert abs(out["restarts"] - ref["iterations"]) <= max(3, ref["iterations"] // 5)
 
 
+@pytest.mark.parametrize("pairs", [0, 1])
+def test_partial_reorthogonalisation_with_and_without_pairs(cfg1_oracle, pairs):
+    """partial_pairs = 1 (default) also projects the step after each fired sketch test; both
+    settings give the reference's eigenpairs with orthonormal Ritz vectors."""
+    A, X0, ref = cfg1_oracle
+    out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8, reorth=native.TRL_REORTH_PARTIAL, partial_pairs=pairs)
+    assert out["converged"]
+    assert np.max(np.abs(out["evals"] - ref["evals"][:10]) / np.abs(ref["evals"][:10])) < 1e-10
+    assert np.max(out["resid"]) < 5e-8
+    X = out["evecs"]
+    assert np.abs(X.T @ X - np.eye(10)).max() < 1e-10
+    assert abs(out["restarts"] - ref["iterations"]) <= max(3, ref["iterations"] // 5)
+
+
 def test_eigenvectors_into_the_callers_buffer(cfg1_oracle):
     """evecs_out (here page-locked, as a repeated caller keeps it) receives exactly what the
     allocating call returns, and is returned itself."""

@@ -697,15 +697,22 @@ __global__ void k_dgks_flag(const double* __restrict__ G_before, const double* _
 }
 
 // flag = ||E||_F^2 > thr2 * trace(G): the sketch S^T W (E) says W's components along the
-// basis exceed thr relative to W's norm (G = W^T W)
+// basis exceed thr relative to W's norm (G = W^T W). With `pair` (a word kept across calls),
+// a step whose test fired also projects the next one: pair = this step's test.
 template <int BS>
-__global__ void k_sketch_flag(const double* __restrict__ E, const double* __restrict__ G, double thr2, int* __restrict__ flag)
+__global__ void k_sketch_flag(const double* __restrict__ E, const double* __restrict__ G, double thr2, int* __restrict__ flag, int* __restrict__ pair)
 {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double e2 = 0.0, tr = 0.0;
   for (int i = 0; i < BS * BS; ++i) e2 = fma(E[i], E[i], e2);
   for (int c = 0; c < BS; ++c) tr += G[c * BS + c];
-  *flag = !(e2 <= thr2 * tr); // NaN counts as loss
+  const int fired = !(e2 <= thr2 * tr); // NaN counts as loss
+  int f = fired;
+  if (pair) {
+    f |= (*pair != 0) ? 2 : 0; // bit 1: forced by the previous step
+    *pair = fired;
+  }
+  *flag = f;
 }
 
 // flag2 = flag1 && (a column kept less than eta of its norm through pass 1)
@@ -1347,7 +1354,8 @@ int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, 
   return st;
 }
 
-int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, const void* S, double thr, double eta, double* G)
+int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int nblk, void* W, int64_t n, int bs, const void* S, double thr, double eta, double* G,
+                                int* pair_state)
 {
   TRL_CHECK_HANDLE(h);
   if (int st = check_common(h, dtype, n, bs)) return st;
@@ -1377,7 +1385,7 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
       st = launch_block_dot_two<T, BS>(h, St, Wt, Wt, n, E);
     }
     if (st) return st;
-    k_sketch_flag<BS><<<1, 32, 0, h->stream>>>(E, Gw0, thr * thr, flag1);
+    k_sketch_flag<BS><<<1, 32, 0, h->stream>>>(E, Gw0, thr * thr, flag1, pair_state);
     if ((st = after_launch(h, "sketch flag"))) return st;
     // both passes only where flagged (decided on the device; their bytes are not credited
     // to the profile because the host does not know whether they ran)
@@ -1405,7 +1413,7 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
       double e2 = 0.0, tr = 0.0;
       for (int i = 0; i < BB; ++i) e2 += eg[i] * eg[i];
       for (int c = 0; c < bs; ++c) tr += eg[BB + c * bs + c];
-      std::fprintf(stderr, "partial nblk %d loss %.3e projected %d second %d\n", nblk, std::sqrt(e2 / tr), fl[0], fl[1]);
+      std::fprintf(stderr, "partial nblk %d loss %.3e projected %d forced %d second %d\n", nblk, std::sqrt(e2 / tr), fl[0] & 1, (fl[0] >> 1) & 1, fl[1]);
     }
   }));
   return st;

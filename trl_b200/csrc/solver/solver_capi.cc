@@ -88,6 +88,7 @@ PhaseOut run_phase(const std::shared_ptr<Context>& ctx, const trl_csr* A, const 
   evp->set_cholqr_passes(p.cholqr_passes);
   evp->set_full_eigenvectors(p.small_eigen_full != 0);
   if (p.partial_threshold > 0.0) evp->set_partial_threshold(p.partial_threshold);
+  evp->set_partial_pairs(p.partial_pairs != 0);
   evp->set_min_eigenvectors(static_cast<std::size_t>(kx) * bs); // the Ritz vectors formed below
   trl::EigensolverParams ep{.nev = p.nev, .ncv = p.ncv, .max_restarts = max_restarts, .tolerance = tol};
   trl::BlockLanczos<EVP, Reorth> lanczos(evp, ep);
@@ -632,7 +633,7 @@ void trl_solve_params_default(trl_solve_params* p)
   p->tol = 1e-8;
   p->alpha = 1.0;
   p->beta = 0.0;
-  p->reorth = TRL_REORTH_PARTIAL; // 96^3 workload: 1.58 s against 2.53 s for TRL_REORTH_CGS_IFNEEDED, same restarts and residuals
+  p->reorth = TRL_REORTH_PARTIAL; // 96^3 workload: 1.25 s against 2.53 s for TRL_REORTH_CGS_IFNEEDED, same restarts and residuals
   p->cholqr_passes = 2;
   p->fp32_tol = 3e-3; // 96^3 workload: 4 FP32 restarts, then filter degree ~1170 of which ~640 in FP32 (0.42 s; 1e-2 and 3e-2 within noise, 1e-3: 0.53 s)
   p->refine_max_restarts = 1000;
@@ -641,6 +642,7 @@ void trl_solve_params_default(trl_solve_params* p)
   p->seed = 42;
   p->refine = TRL_REFINE_CHEBYSHEV;
   p->refine_fp32 = 1;
+  p->partial_pairs = 1; // 96^3 workload: 242 of 3058 steps projected, 1.25 s; 822 steps and 1.56 s without
 }
 
 const char* trl_solver_last_error(void) { return g_err.c_str(); }

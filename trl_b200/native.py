@@ -56,7 +56,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_cholqr": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P]),
     "trl_cuda_cholqr_gram": (C.c_int, [P, C.c_int, P, I64, C.c_int, C.c_int, P, P]),
     "trl_cuda_project_out": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, C.c_int, C.c_double, P]),
-    "trl_cuda_project_out_sketch": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, P, C.c_double, C.c_double, P]),
+    "trl_cuda_project_out_sketch": (C.c_int, [P, C.c_int, P, C.c_int, P, I64, C.c_int, P, C.c_double, C.c_double, P, P]),
     "trl_cuda_spmm": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double]),
     "trl_cuda_csr_norm1": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "trl_cuda_spmm3": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double, C.c_double, P]),
@@ -90,7 +90,8 @@ class trl_solve_params(C.Structure):
                 ("tol", C.c_double), ("alpha", C.c_double), ("beta", C.c_double), ("reorth", C.c_int),
                 ("cholqr_passes", C.c_int), ("fp32_tol", C.c_double), ("refine_max_restarts", C.c_uint),
                 ("want_vectors", C.c_int), ("batching", C.c_int), ("seed", C.c_uint), ("refine", C.c_int),
-                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int), ("small_eigen_full", C.c_int), ("partial_threshold", C.c_double)]
+                ("fp32_ncv", C.c_uint), ("refine_fp32", C.c_int), ("small_eigen_full", C.c_int), ("partial_threshold", C.c_double),
+                ("partial_pairs", C.c_int)]
 
 
 class trl_solve_info(C.Structure):
@@ -244,9 +245,11 @@ class Handle:
         nblk, n, bs = V.shape
         self.check(self.lib.trl_cuda_project_out(self.h, _dtype(V), _ptr(V), nblk, _ptr(W), n, bs, mode, eta, _ptr(G)))
 
-    def project_out_sketch(self, V, W, S, thr: float, G, eta: float = 0.7071067811865476):
+    def project_out_sketch(self, V, W, S, thr: float, G, eta: float = 0.7071067811865476, pair_state=None):
+        """pair_state: optional int32 CUDA tensor (one element, zeroed) kept across the steps
+        of one recurrence; a step whose sketch test fired then also projects the next."""
         nblk, n, bs = V.shape
-        self.check(self.lib.trl_cuda_project_out_sketch(self.h, _dtype(V), _ptr(V), nblk, _ptr(W), n, bs, _ptr(S), thr, eta, _ptr(G)))
+        self.check(self.lib.trl_cuda_project_out_sketch(self.h, _dtype(V), _ptr(V), nblk, _ptr(W), n, bs, _ptr(S), thr, eta, _ptr(G), _ptr(pair_state)))
 
     def cholqr_gram(self, X, passes: int, R, G0):
         n, bs = X.shape
