@@ -307,10 +307,33 @@ __global__ void __launch_bounds__(kThreads) k_block_dot_bulk(const T* __restrict
   }
 }
 
+// Sum of partial[c][e] over the chunks c = s, s + SL, s + 2 SL, ... of one slice. Eight
+// loads are issued before the adds that consume them (a thread issues in order, so each
+// batch is one dependent memory round: ~600 partials take 3 rounds, not 5); eight
+// accumulators, combined in a fixed tree, so the result does not depend on scheduling.
+template <int SL>
+__device__ __forceinline__ double slice_sum(const double* __restrict__ partial, int chunks, int64_t len, int64_t e, int s)
+{
+  constexpr int U = 8;
+  double a[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) a[u] = 0.0;
+  for (int c = s; c < chunks; c += U * SL) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int cu = c + u * SL;
+      v[u] = cu < chunks ? partial[static_cast<int64_t>(cu) * len + e] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) a[u] += v[u];
+  }
+  return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+}
+
 // out[e] = sum_c partial[c][e]: 32 outputs per CTA, 32 slices of the chunk range per output
-// (one warp each) with four independent accumulators each, so that a few hundred partials
-// take two or three dependent load rounds; the slices are combined in a fixed order, so
-// the result does not depend on scheduling.
+// (one warp each, slice_sum); the slices are combined in a fixed order, so the result does
+// not depend on scheduling.
 constexpr int kRedThreads = 1024;
 __global__ void __launch_bounds__(kRedThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out,
                                                                  const int* __restrict__ cond = nullptr)
@@ -320,18 +343,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce_partials(const double* _
   __shared__ double part[SL][33];
   const int o = threadIdx.x & 31, s = threadIdx.x >> 5;
   const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + o;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  if (e < len) {
-    int c = s;
-    for (; c + 3 * SL < chunks; c += 4 * SL) {
-      a0 += partial[static_cast<int64_t>(c) * len + e];
-      a1 += partial[static_cast<int64_t>(c + SL) * len + e];
-      a2 += partial[static_cast<int64_t>(c + 2 * SL) * len + e];
-      a3 += partial[static_cast<int64_t>(c + 3 * SL) * len + e];
-    }
-    for (; c < chunks; c += SL) a0 += partial[static_cast<int64_t>(c) * len + e];
-  }
-  part[s][o] = (a0 + a1) + (a2 + a3);
+  part[s][o] = e < len ? slice_sum<SL>(partial, chunks, len, e, s) : 0.0;
   __syncthreads();
   if (s == 0 && e < len) {
     double t = 0.0;
@@ -760,18 +772,7 @@ __global__ void __launch_bounds__(kRedThreads) k_gram_factor(const double* __res
   if (chunks > 0) {
     for (int e0 = 0; e0 < BS * BS; e0 += 32) {
       const int o = tid & 31, s = tid >> 5, e = e0 + o;
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      if (e < BS * BS) {
-        int c = s;
-        for (; c + 3 * SL < chunks; c += 4 * SL) {
-          a0 += src[static_cast<int64_t>(c) * BS * BS + e];
-          a1 += src[static_cast<int64_t>(c + SL) * BS * BS + e];
-          a2 += src[static_cast<int64_t>(c + 2 * SL) * BS * BS + e];
-          a3 += src[static_cast<int64_t>(c + 3 * SL) * BS * BS + e];
-        }
-        for (; c < chunks; c += SL) a0 += src[static_cast<int64_t>(c) * BS * BS + e];
-      }
-      part[s][o] = (a0 + a1) + (a2 + a3);
+      part[s][o] = e < BS * BS ? slice_sum<SL>(src, chunks, BS * BS, e, s) : 0.0;
       __syncthreads();
       if (s == 0 && e < BS * BS) {
         double t = 0.0;
