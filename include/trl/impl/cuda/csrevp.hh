@@ -67,17 +67,51 @@ private:
   trl_csr desc_{};
 };
 
+/// The operator prepared for repeated SpMMs with block size bs (trl_cuda_op: a sliced-ELL
+/// copy of the CSR matrix, built on the device once). Owns the copy; move-only.
+class SellOp {
+public:
+  SellOp(std::shared_ptr<Context> ctx, const trl_csr* A, int bs)
+      : ctx_(std::move(ctx))
+  {
+    ctx_->flush();
+    ctx_->check(trl_cuda_op_create(ctx_->handle(), A, bs, &op_), "operator preparation");
+  }
+  ~SellOp()
+  {
+    if (op_) trl_cuda_op_destroy(ctx_->handle(), op_);
+  }
+  SellOp(const SellOp&) = delete;
+  SellOp& operator=(const SellOp&) = delete;
+
+  trl_cuda_op get() const { return op_; }
+
+  /// Y_j = alpha A X_j + beta X_j + gamma W_j, j < nb (a direct ABI call: the caller flushes
+  /// the context's recorded operations first when they may touch X, Y or W).
+  void spmm(const void* X, void* Y, int nb, double alpha, double beta, double gamma = 0.0, const void* W = nullptr) const
+  {
+    ctx_->check(trl_cuda_op_spmm(ctx_->handle(), op_, X, Y, nb, alpha, beta, gamma, W), "apply");
+  }
+
+private:
+  std::shared_ptr<Context> ctx_;
+  trl_cuda_op op_ = nullptr;
+};
+
 template <class Storage, unsigned int bs>
 class CSREVP : public EVPBase<Storage, bs> {
 public:
   using Base = EVPBase<Storage, bs>;
   using BlockView = typename Base::BlockView;
 
-  CSREVP(std::shared_ptr<Context> ctx, DeviceCSR<Storage> A, double alpha = 1.0, double beta = 0.0)
+  /// op: the operator prepared for this block size (shared with other users of the same
+  /// matrix); prepared here when null.
+  CSREVP(std::shared_ptr<Context> ctx, DeviceCSR<Storage> A, double alpha = 1.0, double beta = 0.0, std::shared_ptr<const SellOp> op = nullptr)
       : Base(ctx, static_cast<std::size_t>(A.rows()))
       , A_(std::move(A))
       , alpha_(alpha)
       , beta_(beta)
+      , op_(op ? std::move(op) : std::make_shared<const SellOp>(ctx, A_.desc(), static_cast<int>(bs)))
   {
   }
 
@@ -85,7 +119,7 @@ public:
   {
     const std::size_t blk = sizeof(Storage) * this->N * bs;
     this->ctx_->prepare({{X.data_, blk, false}, {Y.data_, blk, true}});
-    this->ctx_->check(trl_cuda_spmm(this->ctx_->handle(), A_.desc(), Base::dtype, X.data_, Y.data_, bs, alpha_, beta_), "apply");
+    op_->spmm(X.data_, Y.data_, 1, alpha_, beta_);
     ++applies_;
   }
 
@@ -97,6 +131,7 @@ public:
 private:
   DeviceCSR<Storage> A_;
   double alpha_, beta_;
+  std::shared_ptr<const SellOp> op_;
   std::uint64_t applies_ = 0;
 };
 

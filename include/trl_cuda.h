@@ -229,6 +229,28 @@ int trl_cuda_spmm3(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X
  * entries are read once for all nb blocks. */
 int trl_cuda_spmm_blocks(trl_cuda_handle h, const trl_csr* A, int dtype, const void* X, void* Y, int bs, int nb, double alpha, double beta, double gamma, const void* W);
 
+/* ---- prepared operator (the solver's SpMM) --------------------------------------------
+ * The operator of CSREVP::apply (examples/sycl/csrevp.hh:159-187,
+ * examples/openmp/csrevp.hh:36-44), converted once for repeated SpMMs with one block size:
+ * a sliced-ELL copy (SELL-C-sigma) in which rows are sorted by length inside windows of 4096
+ * rows and each slice of C rows (C = the rows one warp covers for the dtype and block size)
+ * stores slot j of its C rows as C consecutive indices and values. Each row still sums its
+ * entries in CSR order, as the per-row walk of trl_cuda_spmm_blocks does (bit-identical).
+ * trl_cuda_op_create reads A (device CSR; its arrays are not referenced afterwards) and
+ * allocates the copy from the handle's memory pool; it synchronises the stream once (to size
+ * the copy). The op belongs to the handle's device and is released with
+ * trl_cuda_op_destroy on the same handle. */
+typedef struct trl_cuda_sell_op* trl_cuda_op;
+int trl_cuda_op_create(trl_cuda_handle h, const trl_csr* A, int bs, trl_cuda_op* op);
+int trl_cuda_op_destroy(trl_cuda_handle h, trl_cuda_op op);
+/* Entries stored (padding included), slice height C and longest row (any may be NULL). */
+int trl_cuda_op_info(trl_cuda_op op, int64_t* stored_entries, int* slice_height, int* longest_row);
+/* Y_j = alpha A X_j + beta X_j + gamma W_j for j < nb (nb consecutive n x bs blocks of the
+ * op's dtype; W may be NULL or Y itself, never X). nb = 1, gamma = 0, W = NULL is
+ * CSREVP::apply with the shift beta; the multi-block form is one degree of a Chebyshev
+ * filter on nb blocks. */
+int trl_cuda_op_spmm(trl_cuda_handle h, trl_cuda_op op, const void* X, void* Y, int nb, double alpha, double beta, double gamma, const void* W);
+
 /* Gershgorin interval of alpha*A + beta*I: *host_lo = min_i (c_i - r_i), *host_hi =
  * max_i (c_i + r_i), c_i = alpha*a_ii + beta, r_i = |alpha| sum_{j != i} |a_ij|. Contains
  * every eigenvalue. Synchronises the stream. */

@@ -15,8 +15,9 @@
  *                   kept Ritz vectors (nev/bs + 1 blocks, widened to FP64) to `tol`:
  *                   TRL_REFINE_CHEBYSHEV (default): Rayleigh-Ritz on those vectors
  *                     alternated with Chebyshev-filtered subspace iteration on them (the
- *                     filter damps the spectrum below the kept Ritz values); needs the kept
- *                     Ritz values on one side of zero, else the Lanczos refinement is used;
+ *                     filter damps the spectrum beyond the kept Ritz values: the interval
+ *                     from the far Gershgorin bound to them when they lie on one side of
+ *                     zero, [-b, b] with b their smallest magnitude when they straddle it);
  *                   TRL_REFINE_LANCZOS: a random combination of them starts an FP64
  *                     BlockLanczos solve.
  *

@@ -12,8 +12,10 @@
 
 #include <trl/impl/openmp/evp_base.hh>
 
+#include <chrono>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace trl_oracle {
 
@@ -50,6 +52,17 @@ public:
       for (unsigned j = 0; j < bs; ++j) y[r * bs + j] = static_cast<T>(alpha_) * acc[j] + static_cast<T>(beta_) * x[r * bs + j];
     }
   }
+
+  /// The driver calls solve_small_dense once per restart cycle (lanczos.hh:85): the times of
+  /// those calls mark the end of each cycle (for the CPU baseline's per-cycle timing).
+  std::size_t solve_small_dense(const typename Base::BlockMatrix& B, typename Base::BlockMatrixBlockView beta, std::size_t nev) override
+  {
+    const std::size_t r = Base::solve_small_dense(B, beta, nev);
+    cycle_ends.push_back(std::chrono::steady_clock::now());
+    return r;
+  }
+
+  std::vector<std::chrono::steady_clock::time_point> cycle_ends;
 
 private:
   const std::int32_t* rowptr_;

@@ -23,9 +23,14 @@ OP_DOT, OP_MULT, OP_MULT_T, OP_MULT_ADD, OP_SUB_PROD, OP_SUB, OP_COPY, OP_ZERO =
 _lib = None
 
 
-def build(ref: str = "/root/reference") -> None:
+def reference_root() -> str:
+    """The reference checkout: $TRL_REFERENCE, else the default mount point."""
+    return os.environ.get("TRL_REFERENCE", "/root/reference")
+
+
+def build(ref: str | None = None) -> None:
     """Compile oracle/_ref from the reference sources (needs the reference checkout)."""
-    subprocess.run(["make", "-C", HERE, f"REF={ref}", "-j4"], check=True, stdout=subprocess.DEVNULL)
+    subprocess.run(["make", "-C", HERE, f"REF={ref or reference_root()}", "-j4"], check=True, stdout=subprocess.DEVNULL)
 
 
 def available() -> bool:
@@ -40,7 +45,7 @@ def lib():
         L = C.CDLL(LIB_PATH)
         P = C.c_void_p
         L.oracle_last_error.restype = C.c_char_p
-        L.oracle_solve_csr.argtypes = [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_uint, C.c_double, P, P, P, P, P]
+        L.oracle_solve_csr.argtypes = [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_uint, C.c_double, P, P, P, P, P, P]
         L.oracle_block_view_op.argtypes = [C.c_int, C.c_int, C.c_int64, P, P, P]
         L.oracle_orthonormalize.argtypes = [C.c_int, C.c_int64, P, P]
         L.oracle_solve_small_dense.argtypes = [C.c_int, C.c_uint, P, P, C.c_uint, C.c_double, P, P, P]
@@ -66,20 +71,23 @@ def num_threads() -> int:
 
 def solve_csr(A, bs: int, nev: int, ncv: int, X0: np.ndarray, tol: float = 1e-8, max_restarts: int = 1000,
               alpha: float = 1.0, beta: float = 0.0, ritz: bool = False) -> dict:
-    """Run the reference BlockLanczos (default ModifiedGS) on Y = alpha*A*X + beta*X."""
+    """Run the reference BlockLanczos (default ModifiedGS) on Y = alpha*A*X + beta*X.
+    ``cycle_seconds`` holds the duration of each restart cycle (cycle 1 includes the initial
+    orthonormalisation)."""
     n = A.n
     X0 = np.ascontiguousarray(X0, dtype=np.float64).reshape(n, bs)
     evals = np.zeros(ncv)
     ritz_vecs = np.zeros((n, nev)) if ritz else None
     stats = np.zeros(3, dtype=np.int32)
     secs = np.zeros(1)
+    cycles = np.zeros(max(1, max_restarts))
     rp = np.ascontiguousarray(A.rowptr, dtype=np.int32)
     ci = np.ascontiguousarray(A.colind, dtype=np.int32)
     va = np.ascontiguousarray(A.values, dtype=np.float64)
     _check(lib().oracle_solve_csr(bs, n, _p(rp), _p(ci), _p(va), alpha, beta, nev, ncv, max_restarts, tol, _p(X0),
-                                  _p(evals), _p(ritz_vecs), _p(stats), _p(secs)))
+                                  _p(evals), _p(ritz_vecs), _p(stats), _p(secs), _p(cycles)))
     return {"converged": bool(stats[0]), "iterations": int(stats[1]), "n_op_apply": int(stats[2]),
-            "seconds": float(secs[0]), "evals": evals, "ritz": ritz_vecs}
+            "seconds": float(secs[0]), "evals": evals, "ritz": ritz_vecs, "cycle_seconds": cycles[: int(stats[1])].copy()}
 
 
 def block_view_op(bs: int, op: int, X: np.ndarray, Y: np.ndarray, W: np.ndarray) -> None:

@@ -46,7 +46,7 @@ public:
 
 template <unsigned bs>
 int solve_csr(std::int64_t n, const std::int32_t* rowptr, const std::int32_t* colind, const double* values, double alpha, double beta, unsigned nev, unsigned ncv,
-              unsigned max_restarts, double tol, const double* X0, double* evals_out, double* ritz_out, std::int32_t* stats, double* seconds)
+              unsigned max_restarts, double tol, const double* X0, double* evals_out, double* ritz_out, std::int32_t* stats, double* seconds, double* cycle_seconds)
 {
   using EVP = trl_oracle::CSREVP<double, bs>;
   auto evp = std::make_shared<EVP>(static_cast<std::size_t>(n), rowptr, colind, values, alpha, beta);
@@ -59,6 +59,13 @@ int solve_csr(std::int64_t n, const std::int32_t* rowptr, const std::int32_t* co
   const auto res = lanczos.solve();
   const auto t1 = std::chrono::steady_clock::now();
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (cycle_seconds) { // duration of each restart cycle (cycle 1 includes the first orthonormalisation)
+    auto prev = t0;
+    for (std::size_t i = 0; i < evp->cycle_ends.size() && i < max_restarts; ++i) {
+      cycle_seconds[i] = std::chrono::duration<double>(evp->cycle_ends[i] - prev).count();
+      prev = evp->cycle_ends[i];
+    }
+  }
   if (stats) {
     stats[0] = res.converged ? 1 : 0;
     stats[1] = static_cast<std::int32_t>(res.iterations);
@@ -193,10 +200,11 @@ extern "C" {
 const char* oracle_last_error() { return g_err; }
 
 int oracle_solve_csr(int bs, std::int64_t n, const std::int32_t* rowptr, const std::int32_t* colind, const double* values, double alpha, double beta, unsigned nev,
-                     unsigned ncv, unsigned max_restarts, double tol, const double* X0, double* evals_out, double* ritz_out, std::int32_t* stats, double* seconds)
+                     unsigned ncv, unsigned max_restarts, double tol, const double* X0, double* evals_out, double* ritz_out, std::int32_t* stats, double* seconds,
+                     double* cycle_seconds)
 {
   return guarded([&] {
-    return dispatch_bs<SolveF>(bs, n, rowptr, colind, values, alpha, beta, nev, ncv, max_restarts, tol, X0, evals_out, ritz_out, stats, seconds);
+    return dispatch_bs<SolveF>(bs, n, rowptr, colind, values, alpha, beta, nev, ncv, max_restarts, tol, X0, evals_out, ritz_out, stats, seconds, cycle_seconds);
   });
 }
 

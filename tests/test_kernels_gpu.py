@@ -423,7 +423,9 @@ def _spectrum_matrix(lam, rng):
 def _partial_cases():
     rng = np.random.default_rng(2024)
     cases = []
-    for N, bs in ((40, 8), (160, 4), (384, 8), (448, 16)):
+    # 448: the 8-CTA cluster with shared-memory rows; 512, 640: 16 CTAs, shared-memory rows;
+    # 768, 1024: 16 CTAs, rows in global memory
+    for N, bs in ((40, 8), (160, 4), (384, 8), (448, 16), (512, 16), (640, 16), (768, 16), (1024, 16)):
         M = rng.standard_normal((N, N))
         cases.append((f"random{N}", M + M.T, bs))
     # exact degenerate pairs and a tight cluster at the wanted end (relative gaps 1e-9)
@@ -431,23 +433,25 @@ def _partial_cases():
     lam[-1] = lam[-2] = 5.0
     lam[-10:-2] = 4.0 + 1e-9 * np.arange(8)
     cases.append(("clustered384", _spectrum_matrix(lam, rng), 8))
-    # a thick-restart projected matrix: kept Ritz values on the diagonal, coupling to the
-    # next block, block-tridiagonal below (the structure lanczos.hh:119-150 builds)
-    bs, nblk, kr = 8, 48, 5
-    N = nblk * bs
-    T = np.zeros((N, N))
-    T[: kr * bs, : kr * bs] = np.diag(np.sort(rng.uniform(440, 444, kr * bs))[::-1])
-    for b in range(kr, nblk):
-        D = rng.standard_normal((bs, bs)) * 50 + np.eye(bs) * 200
-        T[b * bs:(b + 1) * bs, b * bs:(b + 1) * bs] = D + D.T
-        if b + 1 < nblk:
-            Bt = np.triu(rng.standard_normal((bs, bs))) * 20
-            T[(b + 1) * bs:(b + 2) * bs, b * bs:(b + 1) * bs] = Bt
-            T[b * bs:(b + 1) * bs, (b + 1) * bs:(b + 2) * bs] = Bt.T
-    C = rng.standard_normal((bs, kr * bs)) * 1e-3
-    T[kr * bs:(kr + 1) * bs, : kr * bs] = C
-    T[: kr * bs, kr * bs:(kr + 1) * bs] = C.T
-    cases.append(("restart384", T, bs))
+    # thick-restart projected matrices: kept Ritz values on the diagonal, coupling to the
+    # next block, block-tridiagonal below (the structure lanczos.hh:119-150 builds); the
+    # second has the shape of the 4M-row bandwidth-stress solve at block size 16 (N = 512,
+    # 100 wanted, 112 kept vectors: the Gram-Schmidt of the kept vectors in global memory)
+    for bs, nblk, kr, nev in ((8, 48, 5, None), (16, 32, 7, 100)):
+        N = nblk * bs
+        T = np.zeros((N, N))
+        T[: kr * bs, : kr * bs] = np.diag(np.sort(rng.uniform(440, 444, kr * bs))[::-1])
+        for b in range(kr, nblk):
+            D = rng.standard_normal((bs, bs)) * 50 + np.eye(bs) * 200
+            T[b * bs:(b + 1) * bs, b * bs:(b + 1) * bs] = D + D.T
+            if b + 1 < nblk:
+                Bt = np.triu(rng.standard_normal((bs, bs))) * 20
+                T[(b + 1) * bs:(b + 2) * bs, b * bs:(b + 1) * bs] = Bt
+                T[b * bs:(b + 1) * bs, (b + 1) * bs:(b + 2) * bs] = Bt.T
+        C = rng.standard_normal((bs, kr * bs)) * 1e-3
+        T[kr * bs:(kr + 1) * bs, : kr * bs] = C
+        T[: kr * bs, kr * bs:(kr + 1) * bs] = C.T
+        cases.append((f"restart{N}", T, bs) + ((nev,) if nev else ()))
     return cases
 
 
@@ -457,12 +461,12 @@ def test_small_eigen_partial_matches_full(cuda_handle, oracle, case):
     against cuSOLVER's full syevd path and the oracle: all eigenvalues, the first kvec
     eigenvectors (residual, orthogonality, and the spanned subspace of each cluster), the
     zeroed remaining columns, and the convergence count."""
-    name, D, bs = case
+    name, D, bs = case[:3]
     rng = np.random.default_rng(7)
     N = D.shape[0]
     T = _block_layout(D, bs, rng)
     beta = np.triu(rng.standard_normal((bs, bs))) * 1e-9
-    nev = 2 * bs
+    nev = case[3] if len(case) > 3 else 2 * bs
     kvec = min(N, (nev // bs + 1) * bs)
     ev_ref, Y_ref, nc_ref = oracle.solve_small_dense(T, beta, bs, nev, tol=1e-7)
     for rep in range(2):  # the second call runs on the workspace the first one left

@@ -200,16 +200,25 @@ def test_fp32_ncv_must_be_a_multiple_of_the_block_size(cfg1_oracle):
         native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_ncv=98)
 
 
-def test_mixed_with_kept_values_on_both_sides_of_zero_uses_lanczos(oracle):
-    """Largest-magnitude eigenvalues of an indefinite matrix: the kept Ritz values straddle
-    zero, no one-sided filter applies, and the refinement falls back to BlockLanczos."""
+@pytest.mark.parametrize("refine", ["chebyshev", "lanczos"])
+def test_mixed_with_kept_values_on_both_sides_of_zero(oracle, refine):
+    """Largest-magnitude eigenvalues of an indefinite matrix (the bandwidth-stress pattern):
+    the kept Ritz values straddle zero. The Chebyshev refinement then filters on [-b, b]
+    centred at zero (b the smallest kept |theta|), amplifying both ends; the Lanczos
+    refinement restarts BlockLanczos. Both agree with the oracle to 1e-10."""
     A = P.zipf_symmetric(20_000, seed=7)
     X0 = P.initial_block(A.n, 8, seed=11)
     ref = oracle.solve_csr(A, 8, 16, 128, X0, tol=1e-10)
-    out = native.solve_csr_host(A, X0, bs=8, nev=16, ncv=128, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4)
+    kind = native.TRL_REFINE_CHEBYSHEV if refine == "chebyshev" else native.TRL_REFINE_LANCZOS
+    out = native.solve_csr_host(A, X0, bs=8, nev=16, ncv=128, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4, refine=kind)
     assert out["converged"]
-    assert out["refine_rounds"] == 0 and out["restarts"] > 0
+    assert np.min(out["evals"]) < 0 < np.max(out["evals"])  # both ends are wanted
+    if refine == "chebyshev":
+        assert out["refine_rounds"] > 0 and out["restarts"] == 0
+    else:
+        assert out["refine_rounds"] == 0 and out["restarts"] > 0
     assert np.max(np.abs(out["evals"] - ref["evals"][:16]) / np.abs(ref["evals"][:16])) < 1e-10
+    assert out["max_theta_residual"] < 1e-10
 
 
 def test_fp32_mode_accuracy_is_stated(cfg1_oracle):

@@ -28,8 +28,9 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 # The image exports CXX pointing at a wrapper compiler; the system g++ is used explicitly.
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["context.cu", "blockvec.cu", "spmm.cu", "small.cu"]
-DEFAULT_REF = "/root/reference"
+CU_SOURCES = ["context.cu", "blockvec.cu", "spmm.cu", "sell.cu", "small.cu"]
+# the header-only reference checkout (build time only): $TRL_REFERENCE or the default mount
+DEFAULT_REF = os.environ.get("TRL_REFERENCE", "/root/reference")
 
 
 def _newer(target: str, deps: list[str]) -> bool:

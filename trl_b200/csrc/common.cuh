@@ -179,6 +179,79 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// ---- vector loads shared by the SpMM kernels (spmm.cu, sell.cu) ---------------------------
+namespace trl_detail {
+
+template <typename T, int VEC>
+struct VecT;
+template <>
+struct VecT<double, 1> {
+  using type = double;
+};
+template <>
+struct VecT<double, 2> {
+  using type = double2;
+};
+template <>
+struct VecT<float, 1> {
+  using type = float;
+};
+template <>
+struct VecT<float, 2> {
+  using type = float2;
+};
+template <>
+struct VecT<float, 4> {
+  using type = float4;
+};
+
+template <typename T, int VEC>
+__device__ __forceinline__ void load_vec(const T* p, T (&out)[VEC])
+{
+  using V = typename VecT<T, VEC>::type;
+  const V v = __ldg(reinterpret_cast<const V*>(p));
+  if constexpr (VEC == 1) {
+    out[0] = reinterpret_cast<const T*>(&v)[0];
+  }
+  else {
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) out[i] = reinterpret_cast<const T*>(&v)[i];
+  }
+}
+
+template <typename T, int VEC>
+__device__ __forceinline__ void store_vec(T* p, const T (&in)[VEC])
+{
+  using V = typename VecT<T, VEC>::type;
+  V v;
+#pragma unroll
+  for (int i = 0; i < VEC; ++i) reinterpret_cast<T*>(&v)[i] = in[i];
+  *reinterpret_cast<V*>(p) = v;
+}
+
+// The CSR stream is read once: load it without allocating in L1, which keeps L1 for the
+// X rows that neighbouring rows gather again.
+__device__ __forceinline__ int ld_stream(const int32_t* p)
+{
+  int v;
+  asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p)
+{
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p)
+{
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
+} // namespace trl_detail
+
 #define TRL_CHECK_HANDLE(h)                                                                                                                                                                            \
   do {                                                                                                                                                                                                 \
     if (!(h)) return TRL_EINVAL;                                                                                                                                                                       \

@@ -13,6 +13,7 @@
 
 #include <cfloat>
 #include <cstring>
+#include <mutex>
 
 namespace {
 
@@ -260,8 +261,8 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
 // (|theta| descending), which is all the driver reads (the kept blocks, lanczos.hh:105-131).
 // For 3 <= N <= kTriMaxN and kvec <= kTriMaxVec it runs without cuSOLVER:
 //  1. k_tridiag: Householder tridiagonalisation Q^T A Q = T in ONE thread-block cluster of
-//     kTriC CTAs. A (full symmetric storage) is distributed over the CTAs' shared memory by
-//     rows (row g on CTA g % kTriC); each step exchanges the Householder column and the
+//     8 or 16 CTAs. A (full symmetric storage) is distributed over the CTAs by rows (row g
+//     on CTA g % C, in its shared memory up to N = 640); each step exchanges the Householder column and the
 //     vector p = tau A v through distributed shared memory, two cluster barriers per step.
 //     (cuSOLVER's tridiagonalisation of the same matrix is a sequence of small kernels, about
 //     3.7 ms at N = 384 on B200.)
@@ -282,18 +283,25 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
 
 namespace {
 
-constexpr int kTriC = 8;           // CTAs in the tridiagonalisation cluster (portable size)
+// The tridiagonalisation runs in one thread-block cluster; its rows live in the CTAs' shared
+// memory while they fit, in global memory (the dense copy it works on, L2-resident) beyond:
+//   N <= kTriMaxN8      8 CTAs (portable cluster size), rows in shared memory;
+//   N <= kTriMaxN16    16 CTAs (non-portable cluster size), rows in shared memory;
+//   N <= kTriMaxN      16 CTAs, rows in global memory.
+// Rows per CTA * N * 8 B must fit one CTA's shared memory (227 KB) for the first two.
 constexpr int kTriThreads = 512;
-constexpr int kTriMaxN = 448;      // rows per CTA * N * 8 B must fit one CTA's shared memory
-constexpr int kTriMaxVec = 128;    // vectors by inverse iteration
+constexpr int kTriMaxN8 = 448;
+constexpr int kTriMaxN16 = 640;
+constexpr int kTriMaxN = 1024;
+constexpr int kTriMaxVec = 256;    // vectors by inverse iteration
 constexpr int kTriIters = 3;       // inverse-iteration sweeps
 constexpr int kBisectMaxN = kTriMaxN;
-constexpr size_t kTriGsMaxBytes = 200 * 1024; // the K vectors of N entries in one CTA's shared memory
+constexpr size_t kTriGsMaxBytes = 200 * 1024; // the K vectors of N entries in one CTA's shared memory (else in global memory)
 
-size_t tridiag_smem(int N)
+size_t tridiag_smem(int N, int C, bool global_rows)
 {
-  const int RB = (N + kTriC - 1) / kTriC;
-  return sizeof(double) * (static_cast<size_t>(RB) * N + 4 * N + 2 * kTriC * (kTriThreads / 32) + 8);
+  const int RB = (N + C - 1) / C;
+  return sizeof(double) * ((global_rows ? 0 : static_cast<size_t>(RB) * N) + 4 * N + 2 * C * (kTriThreads / 32) + 8);
 }
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -344,70 +352,76 @@ __device__ __forceinline__ void stage(double* dst, const double* __restrict__ sr
 
 // A: N x N symmetric (full storage). Outputs: d[N], e[N-1] of T = Q^T A Q with
 // Q = H_0 ... H_{N-3}, H_k = I - tau_k v_k v_k^T, v_k stored in refl[k*N + k+1 .. N-1]
-// (refl[k*N + k+1] = 1).
+// (refl[k*N + k+1] = 1). Row g belongs to CTA g % C of the cluster (C CTAs); with
+// kGlobalRows it is updated in place in A (only its owner reads or writes it, so the CTA's
+// own barriers order the accesses), otherwise it is copied into the owner's shared memory.
 // Exchange by pushing: before each cluster barrier every CTA stores its entries of the
 // Householder column (then of p = tau A v) and its per-warp partial sums into the shared
 // memory of every CTA of the cluster (st.shared::cluster through map_shared_rank); after
 // the barrier each CTA reads only its own shared memory. Every CTA reduces the same
 // partials in the same order, so all hold bit-identical scalars. A buffer filled at one
 // barrier is read before the next one, which its next writers wait for.
-__global__ void __cluster_dims__(kTriC, 1, 1) __launch_bounds__(kTriThreads, 1)
-    k_tridiag(const double* __restrict__ A, int N, double* __restrict__ dout, double* __restrict__ eout, double* __restrict__ tau_out, double* __restrict__ refl)
+template <int C, bool kGlobalRows>
+__global__ void __launch_bounds__(kTriThreads, 1)
+    k_tridiag(double* __restrict__ A, int N, double* __restrict__ dout, double* __restrict__ eout, double* __restrict__ tau_out, double* __restrict__ refl)
 {
   namespace cg = cooperative_groups;
   constexpr int NW = kTriThreads / 32;
-  constexpr int NP = kTriC * NW; // partials per exchange
-  static_assert(NP == 128, "partials are reduced as 4 per lane");
+  constexpr int NP = C * NW; // partials per exchange
+  static_assert(NP % 32 == 0, "partials are reduced as NP / 32 per lane");
   cg::cluster_group cluster = cg::this_cluster();
   const int r = static_cast<int>(cluster.block_rank());
-  const int RB = (N + kTriC - 1) / kTriC;
+  const int RB = (N + C - 1) / C;
   extern __shared__ __align__(16) double sm[];
-  double* rows = sm;              // RB x N, local row l = global row r + kTriC * l
-  double* xfull = rows + RB * N;  // N: column k below the diagonal (pushed by the owners)
+  double* const rows = kGlobalRows ? nullptr : sm; // RB x N, local row l = global row r + C * l
+  double* xfull = sm + (kGlobalRows ? 0 : RB * N); // N: column k below the diagonal (pushed by the owners)
   double* pfull = xfull + N;      // N: p (pushed by the owners)
   double* vfull = pfull + N;      // N
   double* wfull = vfull + N;      // N
   double* part = wfull + N;       // NP sums of squares (slot rank * NW + warp), then x0
   double* part2 = part + NP + 8;  // NP partial p.v
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  auto row = [&](int l) -> double* { return kGlobalRows ? A + static_cast<size_t>(r + C * l) * N : rows + static_cast<size_t>(l) * N; };
 
   auto local_sum = [&](const double* slot) {
     double s = 0.0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) s += slot[lane + 32 * q];
+    for (int q = 0; q < NP / 32; ++q) s += slot[lane + 32 * q];
     return warp_sum(s);
   };
   // store v at offset `at` of `buf` in every CTA of the cluster
   auto push = [&](double* buf, int at, double v) {
 #pragma unroll
-    for (int q = 0; q < kTriC; ++q) cluster.map_shared_rank(buf, q)[at] = v;
+    for (int q = 0; q < C; ++q) cluster.map_shared_rank(buf, q)[at] = v;
   };
 
-  for (int l = 0; l < RB; ++l) {
-    const int g = r + kTriC * l;
-    if (g < N) stage(rows + l * N, A + static_cast<size_t>(g) * N, N);
-    else
-      for (int j = tid; j < N; j += kTriThreads) rows[l * N + j] = 0.0;
+  if (!kGlobalRows) {
+    for (int l = 0; l < RB; ++l) {
+      const int g = r + C * l;
+      if (g < N) stage(rows + l * N, A + static_cast<size_t>(g) * N, N);
+      else
+        for (int j = tid; j < N; j += kTriThreads) rows[l * N + j] = 0.0;
+    }
   }
   cluster.sync(); // every CTA is running before any pushes into it
 
   for (int k = 0; k < N - 2; ++k) {
-    const int l0 = (k + 1 - r + kTriC - 1) / kTriC > 0 ? (k + 1 - r + kTriC - 1) / kTriC : 0; // first local row > k
-    if (r == k % kTriC && tid == 0) dout[k] = rows[(k / kTriC) * N + k];
+    const int l0 = (k + 1 - r + C - 1) / C > 0 ? (k + 1 - r + C - 1) / C : 0; // first local row > k
+    if (r == k % C && tid == 0) dout[k] = row(k / C)[k];
     // ---- phase A: push this CTA's entries of x = A[k+1:, k] and its partial sum of squares
     {
       double ssq = 0.0;
       if (tid < RB - l0) {
-        const int l = l0 + tid, g = r + kTriC * l;
+        const int l = l0 + tid, g = r + C * l;
         if (g < N) {
-          const double x = rows[l * N + k];
+          const double x = row(l)[k];
           push(xfull, g, x);
           if (g > k + 1) ssq = x * x;
         }
       }
       ssq = warp_sum(ssq);
-      if (lane < kTriC) cluster.map_shared_rank(part, lane)[r * NW + warp] = ssq;
-      if (tid == 0 && r == (k + 1) % kTriC) push(part, NP, rows[((k + 1) / kTriC) * N + k]);
+      if (lane < C) cluster.map_shared_rank(part, lane)[r * NW + warp] = ssq;
+      if (tid == 0 && r == (k + 1) % C) push(part, NP, row((k + 1) / C)[k]);
     }
     cluster.sync(); // #1
     const double xnorm2 = local_sum(part);
@@ -420,7 +434,7 @@ __global__ void __cluster_dims__(kTriC, 1, 1) __launch_bounds__(kTriThreads, 1)
     }
     for (int j = k + 1 + tid; j < N; j += kTriThreads) vfull[j] = (j == k + 1) ? 1.0 : xfull[j] * scale;
     __syncthreads();
-    if (r == k % kTriC) {
+    if (r == k % C) {
       for (int j = k + 1 + tid; j < N; j += kTriThreads) refl[static_cast<size_t>(k) * N + j] = vfull[j];
       if (tid == 0) {
         tau_out[k] = tau;
@@ -431,15 +445,16 @@ __global__ void __cluster_dims__(kTriC, 1, 1) __launch_bounds__(kTriThreads, 1)
     // partial p.v
     double pv = 0.0;
     for (int l = l0 + warp; l < RB; l += NW) {
-      const int g = r + kTriC * l;
+      const int g = r + C * l;
       if (g >= N) break;
+      const double* rl = row(l);
       double s = 0.0;
-      for (int j = k + 1 + lane; j < N; j += 32) s = fma(rows[l * N + j], vfull[j], s);
+      for (int j = k + 1 + lane; j < N; j += 32) s = fma(rl[j], vfull[j], s);
       s = warp_sum(s) * tau;
-      if (lane < kTriC) cluster.map_shared_rank(pfull, lane)[g] = s;
+      if (lane < C) cluster.map_shared_rank(pfull, lane)[g] = s;
       pv = fma(s, vfull[g], pv);
     }
-    if (lane < kTriC) cluster.map_shared_rank(part2, lane)[r * NW + warp] = pv;
+    if (lane < C) cluster.map_shared_rank(part2, lane)[r * NW + warp] = pv;
     cluster.sync(); // #2
     const double K = 0.5 * tau * local_sum(part2);
     for (int j = k + 1 + tid; j < N; j += kTriThreads) wfull[j] = pfull[j] - K * vfull[j];
@@ -447,19 +462,20 @@ __global__ void __cluster_dims__(kTriC, 1, 1) __launch_bounds__(kTriThreads, 1)
     // ---- phase D: rank-2 update of this CTA's trailing rows (warp per row)
     if (tau != 0.0) {
       for (int l = l0 + warp; l < RB; l += NW) {
-        const int g = r + kTriC * l;
+        const int g = r + C * l;
         if (g >= N) break;
+        double* rl = row(l);
         const double vg = vfull[g], wg = wfull[g];
-        for (int j = k + 1 + lane; j < N; j += 32) rows[l * N + j] -= vg * wfull[j] + wg * vfull[j];
+        for (int j = k + 1 + lane; j < N; j += 32) rl[j] -= vg * wfull[j] + wg * vfull[j];
       }
     }
     __syncthreads();
   }
   if (tid == 0) {
-    if (N >= 2 && r == (N - 2) % kTriC) dout[N - 2] = rows[((N - 2) / kTriC) * N + N - 2];
-    if (r == (N - 1) % kTriC) {
-      dout[N - 1] = rows[((N - 1) / kTriC) * N + N - 1];
-      if (N >= 2) eout[N - 2] = rows[((N - 1) / kTriC) * N + N - 2];
+    if (N >= 2 && r == (N - 2) % C) dout[N - 2] = row((N - 2) / C)[N - 2];
+    if (r == (N - 1) % C) {
+      dout[N - 1] = row((N - 1) / C)[N - 1];
+      if (N >= 2) eout[N - 2] = row((N - 1) / C)[N - 2];
     }
   }
   cluster.sync(); // no CTA leaves while another may still store into its shared memory
@@ -652,15 +668,18 @@ __global__ void __launch_bounds__(32) k_tri_solve(int N, const double* __restric
 }
 
 // classical Gram-Schmidt applied twice, column by column in ascending eigenvalue order, on
-// the K vectors held in shared memory; one CTA of kTriThreads threads
+// the K vectors held in shared memory (kGlobal: in place in Z, for K x N beyond one CTA's
+// shared memory); one CTA of kTriThreads threads
+template <bool kGlobal>
 __global__ void __launch_bounds__(kTriThreads) k_tri_gs(int N, int K, double* __restrict__ Z)
 {
-  extern __shared__ __align__(16) double zs[]; // K x N
+  extern __shared__ __align__(16) double zsm[]; // K x N
+  double* const zs = kGlobal ? Z : zsm;
   __shared__ double coef[kTriMaxVec];
   __shared__ double red[32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = kTriThreads / 32;
-  stage(zs, Z, K * N);
+  if (!kGlobal) stage(zs, Z, K * N);
   __syncthreads();
   for (int j = 0; j < K; ++j) {
     double* zj = zs + static_cast<size_t>(j) * N;
@@ -687,7 +706,8 @@ __global__ void __launch_bounds__(kTriThreads) k_tri_gs(int N, int K, double* __
     for (int n = tid; n < N; n += kTriThreads) zj[n] *= inv;
     __syncthreads();
   }
-  for (int idx = tid; idx < K * N; idx += kTriThreads) Z[idx] = zs[idx];
+  if (!kGlobal)
+    for (int idx = tid; idx < K * N; idx += kTriThreads) Z[idx] = zs[idx];
 }
 
 // Back-transform X = Q Z, Q = H_0 ... H_{N-3}, in chunks of kWyRows reflectors: a chunk
@@ -855,6 +875,71 @@ __global__ void k_zero_cols(double* __restrict__ Y, int nblk, int bs, int K)
   }
 }
 
+using TriKernel = void (*)(double*, int, double*, double*, double*, double*);
+
+struct TriVariant {
+  TriKernel fn;
+  int C;       // CTAs in the cluster
+  bool global; // rows in global memory
+  int max_n;
+};
+
+constexpr TriVariant kTriVariants[] = {
+    {k_tridiag<8, false>, 8, false, kTriMaxN8},
+    {k_tridiag<16, false>, 16, false, kTriMaxN16},
+    {k_tridiag<16, true>, 16, true, kTriMaxN},
+    {k_tridiag<8, true>, 8, true, kTriMaxN},
+};
+constexpr int kNumTriVariants = sizeof(kTriVariants) / sizeof(kTriVariants[0]);
+
+void tri_config(const TriVariant& v, int N, cudaStream_t stream, cudaLaunchConfig_t& cfg, cudaLaunchAttribute& attr)
+{
+  cfg = cudaLaunchConfig_t{};
+  cfg.gridDim = dim3(v.C);
+  cfg.blockDim = dim3(kTriThreads);
+  cfg.dynamicSmemBytes = tridiag_smem(N, v.C, v.global);
+  cfg.stream = stream;
+  attr = cudaLaunchAttribute{};
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = v.C;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+}
+
+// The first variant that takes N and can be resident on `device`, or null. Checked once per
+// device: function attributes belong to the current device.
+const TriVariant* tri_variant(int device, int N)
+{
+  static int ok[64][kNumTriVariants];
+  static bool checked[64];
+  static std::mutex lock;
+  std::lock_guard<std::mutex> g(lock);
+  if (!checked[device]) {
+    checked[device] = true;
+    const bool common = cudaFuncSetAttribute(k_tri_gs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTriGsMaxBytes)) == cudaSuccess &&
+                        cudaFuncSetAttribute(k_tri_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * (kFactorRows + 1) * kTriMaxN)) == cudaSuccess &&
+                        cudaFuncSetAttribute(k_tri_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * kFactorRows * kTriMaxN)) == cudaSuccess &&
+                        cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * (kWyRows + kWyVecs) * kTriMaxN)) == cudaSuccess &&
+                        cudaFuncSetAttribute(k_wy_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * kWyRows * kTriMaxN)) == cudaSuccess;
+    for (int i = 0; i < kNumTriVariants && common; ++i) {
+      const TriVariant& v = kTriVariants[i];
+      if (cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tridiag_smem(v.max_n, v.C, v.global))) != cudaSuccess) continue;
+      if (v.C > 8 && cudaFuncSetAttribute(v.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) continue;
+      cudaLaunchConfig_t cfg{};
+      cudaLaunchAttribute attr{};
+      tri_config(v, v.max_n, nullptr, cfg, attr);
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, v.fn, &cfg) == cudaSuccess && clusters > 0) ok[device][i] = 1;
+    }
+    cudaGetLastError();
+  }
+  for (int i = 0; i < kNumTriVariants; ++i)
+    if (ok[device][i] && N <= kTriVariants[i].max_n) return &kTriVariants[i];
+  return nullptr;
+}
+
 } // namespace
 
 extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, int nblk, int bs, const double* beta, int nev, double tol, int kvec, double* evals, double* evecs,
@@ -864,37 +949,9 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   if (!valid_bs(bs) || nblk <= 0 || !T || !beta || !evals || !evecs || !host_evals || !host_nconv) return set_error(h, TRL_EINVAL, "bad small_eigen arguments");
   const int N = nblk * bs;
   if (kvec < 0 || kvec > N) return set_error(h, TRL_EINVAL, "kvec %d outside [0, %d]", kvec, N);
-  // per device (function attributes are set for the current device): whether a kTriC-CTA
-  // cluster with the shared memory of N = kTriMaxN can be resident
-  static int cluster_ok_dev[64];
-  static bool cluster_checked[64];
   if (h->device < 0 || h->device >= 64) return set_error(h, TRL_EINVAL, "device index %d", h->device);
-  int& cluster_ok = cluster_ok_dev[h->device];
-  if (!cluster_checked[h->device]) {
-    cluster_checked[h->device] = true;
-    cluster_ok = 0;
-    const size_t smem = tridiag_smem(kTriMaxN);
-    if (cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) == cudaSuccess &&
-        cudaFuncSetAttribute(k_tri_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTriGsMaxBytes)) == cudaSuccess &&
-        cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * (kWyRows + kWyVecs) * kTriMaxN)) == cudaSuccess &&
-        cudaFuncSetAttribute(k_wy_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(sizeof(double) * kWyRows * kTriMaxN)) == cudaSuccess) {
-      cudaLaunchConfig_t cfg{};
-      cfg.gridDim = dim3(kTriC);
-      cfg.blockDim = dim3(kTriThreads);
-      cfg.dynamicSmemBytes = smem;
-      cudaLaunchAttribute attr{};
-      attr.id = cudaLaunchAttributeClusterDimension;
-      attr.val.clusterDim.x = kTriC;
-      attr.val.clusterDim.y = 1;
-      attr.val.clusterDim.z = 1;
-      cfg.attrs = &attr;
-      cfg.numAttrs = 1;
-      int clusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&clusters, k_tridiag, &cfg) == cudaSuccess && clusters > 0) cluster_ok = 1;
-    }
-    cudaGetLastError();
-  }
-  if (N < 3 || N > kTriMaxN || kvec > kTriMaxVec || sizeof(double) * N * (kvec > 0 ? kvec : 1) > kTriGsMaxBytes || cluster_ok != 1) {
+  const TriVariant* tv = tri_variant(h->device, N);
+  if (N < 3 || kvec > kTriMaxVec || !tv) {
     if (int st = trl_cuda_small_eigen(h, T, nblk, bs, beta, nev, tol, evals, evecs, host_evals, host_nconv)) return st;
     k_zero_cols<<<grid_for(h, static_cast<int64_t>(N) * N, 256, 4), 256, 0, h->stream>>>(evecs, nblk, bs, kvec);
     return after_launch(h, "zero columns");
@@ -928,8 +985,13 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, A);
   if (int st = after_launch(h, "assemble")) return st;
   cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream);
-  k_tridiag<<<kTriC, kTriThreads, tridiag_smem(N), h->stream>>>(A, N, d, e, tau, refl);
-  if (int st = after_launch(h, "tridiagonalise")) return st;
+  {
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr{};
+    tri_config(*tv, N, h->stream, cfg, attr);
+    cudaLaunchKernelEx(&cfg, tv->fn, A, N, d, e, tau, refl);
+    if (int st = after_launch(h, "tridiagonalise")) return st;
+  }
   k_bisect<<<(N + 7) / 8, 256, 0, h->stream>>>(d, e, N, w);
   if (int st = after_launch(h, "bisect")) return st;
   k_rank<<<(N + 255) / 256, 256, 0, h->stream>>>(w, N, perm, evals, flags, h->d_status);
@@ -942,7 +1004,8 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
     k_tri_solve<<<K, 32, sizeof(double) * (kFactorRows + 1) * N, h->stream>>>(N, F, Z);
     if (int st = after_launch(h, "inverse iteration")) return st;
   }
-  k_tri_gs<<<1, kTriThreads, sizeof(double) * NK, h->stream>>>(N, K, Z);
+  if (sizeof(double) * NK > kTriGsMaxBytes) k_tri_gs<true><<<1, kTriThreads, 0, h->stream>>>(N, K, Z);
+  else k_tri_gs<false><<<1, kTriThreads, sizeof(double) * NK, h->stream>>>(N, K, Z);
   if (int st = after_launch(h, "gram-schmidt")) return st;
   const int nch = (N - 2 + kWyRows - 1) / kWyRows;
   k_wy_factor<<<nch, 256, sizeof(double) * kWyRows * N, h->stream>>>(refl, tau, N, Tw);

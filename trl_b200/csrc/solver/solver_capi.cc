@@ -35,6 +35,7 @@ thread_local std::string g_err;
 using trl::cuda::Context;
 using trl::cuda::DeviceBuffer;
 using trl::cuda::DeviceCSR;
+using trl::cuda::SellOp;
 
 static_assert(trl::Eigenproblem<trl::cuda::CSREVP<double, 8>>);
 static_assert(trl::Eigenproblem<trl::cuda::CSREVP<float, 8>>);
@@ -79,12 +80,12 @@ struct PhaseOut {
 /// Runs BlockLanczos<CSREVP<Storage,bs>, Reorth> from the device block X0 and writes the
 /// first `kx` blocks of Ritz vectors (block layout, Storage) to ritz_out.
 template <class Storage, unsigned bs, class Reorth>
-PhaseOut run_phase(const std::shared_ptr<Context>& ctx, const trl_csr* A, const trl_solve_params& p, unsigned max_restarts, double tol, const Storage* X0, unsigned kx,
-                   Storage* ritz_out)
+PhaseOut run_phase(const std::shared_ptr<Context>& ctx, const trl_csr* A, const std::shared_ptr<const SellOp>& op, const trl_solve_params& p, unsigned max_restarts, double tol,
+                   const Storage* X0, unsigned kx, Storage* ritz_out)
 {
   using EVP = trl::cuda::CSREVP<Storage, bs>;
   auto Adev = DeviceCSR<Storage>::wrap(A->n, A->nnz, A->rowptr, A->colind, static_cast<const Storage*>(A->values));
-  auto evp = std::make_shared<EVP>(ctx, std::move(Adev), p.alpha, p.beta);
+  auto evp = std::make_shared<EVP>(ctx, std::move(Adev), p.alpha, p.beta, op);
   evp->set_cholqr_passes(p.cholqr_passes);
   evp->set_full_eigenvectors(p.small_eigen_full != 0);
   if (p.partial_threshold > 0.0) evp->set_partial_threshold(p.partial_threshold);
@@ -126,15 +127,15 @@ PhaseOut run_phase(const std::shared_ptr<Context>& ctx, const trl_csr* A, const 
 }
 
 template <class Storage, unsigned bs>
-PhaseOut run_phase_r(const std::shared_ptr<Context>& ctx, const trl_csr* A, const trl_solve_params& p, unsigned max_restarts, double tol, const Storage* X0, unsigned kx,
-                     Storage* ritz_out)
+PhaseOut run_phase_r(const std::shared_ptr<Context>& ctx, const trl_csr* A, const std::shared_ptr<const SellOp>& op, const trl_solve_params& p, unsigned max_restarts, double tol,
+                     const Storage* X0, unsigned kx, Storage* ritz_out)
 {
   switch (p.reorth) {
-  case TRL_REORTH_MGS: return run_phase<Storage, bs, trl::ModifiedGS>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
-  case TRL_REORTH_CGS2: return run_phase<Storage, bs, trl::cuda::BlockCGS2>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
-  case TRL_REORTH_CGS1: return run_phase<Storage, bs, trl::cuda::BlockCGS1>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
-  case TRL_REORTH_PARTIAL: return run_phase<Storage, bs, trl::cuda::BlockCGSPartial>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
-  default: return run_phase<Storage, bs, trl::cuda::BlockCGSIfNeeded>(ctx, A, p, max_restarts, tol, X0, kx, ritz_out);
+  case TRL_REORTH_MGS: return run_phase<Storage, bs, trl::ModifiedGS>(ctx, A, op, p, max_restarts, tol, X0, kx, ritz_out);
+  case TRL_REORTH_CGS2: return run_phase<Storage, bs, trl::cuda::BlockCGS2>(ctx, A, op, p, max_restarts, tol, X0, kx, ritz_out);
+  case TRL_REORTH_CGS1: return run_phase<Storage, bs, trl::cuda::BlockCGS1>(ctx, A, op, p, max_restarts, tol, X0, kx, ritz_out);
+  case TRL_REORTH_PARTIAL: return run_phase<Storage, bs, trl::cuda::BlockCGSPartial>(ctx, A, op, p, max_restarts, tol, X0, kx, ritz_out);
+  default: return run_phase<Storage, bs, trl::cuda::BlockCGSIfNeeded>(ctx, A, op, p, max_restarts, tol, X0, kx, ritz_out);
   }
 }
 
@@ -171,12 +172,15 @@ struct RefineOut {
 template <unsigned bs>
 class ChebyshevRefinement {
 public:
-  /// A32 (may be null): the FP32 copy of the operator, for the FP32 filter rounds.
-  ChebyshevRefinement(std::shared_ptr<Context> ctx, const trl_csr* A, const trl_csr* A32, const trl_solve_params& p, unsigned kr)
+  /// A: the FP64 operator (CSR, for its Gershgorin bounds) and op64 its prepared copy;
+  /// op32 (may be null): the prepared FP32 copy, for the FP32 filter rounds.
+  ChebyshevRefinement(std::shared_ptr<Context> ctx, const trl_csr* A, std::shared_ptr<const SellOp> op64, std::shared_ptr<const SellOp> op32, const trl_solve_params& p,
+                      unsigned kr)
       : ctx_(std::move(ctx))
       , h_(ctx_->handle())
       , A_(A)
-      , A32_(A32)
+      , op64_(std::move(op64))
+      , op32_(std::move(op32))
       , p_(p)
       , kr_(kr)
       , n_(A->n)
@@ -190,8 +194,8 @@ public:
       , Z_(ctx_, sizeof(double) * kr * kr * bs * bs)
       , ev_(ctx_, sizeof(double) * kr * bs)
       , small_(ctx_, sizeof(double) * 4 * bs * bs)
-      , X32_(ctx_, A32 ? sizeof(float) * blk_ * kr : 0)
-      , Y32_(ctx_, A32 ? sizeof(float) * blk_ * kr : 0)
+      , X32_(ctx_, op32_ ? sizeof(float) * blk_ * kr : 0)
+      , Y32_(ctx_, op32_ ? sizeof(float) * blk_ * kr : 0)
   {
   }
 
@@ -206,7 +210,7 @@ public:
     double* spare = static_cast<double*>(Y_.get());
     orthonormalize(cur);
     const unsigned N = kr_ * bs;
-    bool use32 = A32_ != nullptr;
+    bool use32 = op32_ != nullptr;
     double prev_res = 0.0; // residual at the start of the last FP32 round
     for (unsigned round = 0; round < kMaxRounds; ++round) {
       std::vector<double> theta = rayleigh_ritz(cur, spare); // cur <- Ritz vectors (in spare, swapped)
@@ -219,21 +223,25 @@ public:
         return finish(out, cur, X);
       }
       if (round + 1 == kMaxRounds) break; // leave the last Rayleigh-Ritz vectors in place
-      // orientation: the kept Ritz values must lie on one side of zero
+      // orientation. Kept Ritz values on one side of zero: filter s * op (s the sign of the
+      // kept values) on the damped interval [a, b], a the far Gershgorin bound, b the kept
+      // value nearest the rest of the spectrum. Kept values on both sides of zero (the
+      // largest-magnitude eigenvalues of an indefinite operator): the interval [-b, b], b the
+      // smallest kept |theta|, centred at zero, so that T_d(op / b) amplifies both ends alike
+      // (|T_d(x / b)| grows with |x| outside it).
       double tmin = theta[0], tmax = theta[0];
       for (double t : theta) {
         tmin = std::min(tmin, t);
         tmax = std::max(tmax, t);
       }
-      if (!(tmin > 0.0) && !(tmax < 0.0)) return finish(out, cur, X); // not applicable
-      const double s = tmin > 0.0 ? 1.0 : -1.0;       // filter s * op: the kept end is the top
-      // damped interval [a, b] in s-coordinates; wanted top end above b
-      const double a = s > 0 ? lo : -hi;
-      const double b = s > 0 ? tmin : -tmax;
-      const double top = s * theta[0];                                           // largest |theta|
-      const double worst = s * theta[std::min<std::size_t>(p_.nev, N) - 1];     // smallest wanted
+      const bool one_sided = tmin > 0.0 || tmax < 0.0;
+      const double s = one_sided && tmax < 0.0 ? -1.0 : 1.0;
+      const double b = one_sided ? (s > 0 ? tmin : -tmax) : std::abs(theta[N - 1]);
+      const double a = one_sided ? (s > 0 ? lo : -hi) : -b;
+      const double top = std::abs(theta[0]);                                          // largest |theta|
+      const double worst = std::abs(theta[std::min<std::size_t>(p_.nev, N) - 1]);     // smallest wanted
       const double c = 0.5 * (a + b), e = 0.5 * (b - a);
-      if (!(e > 0.0) || !(worst > b)) return finish(out, cur, X);
+      if (!(e > 0.0) || !(worst > b)) return finish(out, cur, X); // not applicable
       const double xw = (worst - c) / e, xt = (top - c) / e;
       const double rw = std::acosh(xw), rt = std::acosh(std::max(xt, xw));
       // FP32 rounds while the residual is above what FP32 vectors resolve and FP32 rounds
@@ -251,14 +259,16 @@ public:
       const double target = use32 ? std::max(0.1 * p_.tol, kFp32Target) : 0.1 * p_.tol;
       const double need_all = std::log(2.0 * std::max(res / target, 2.0));
       const double need = std::min(need_all, std::log(100.0));
-      const unsigned d_all = static_cast<unsigned>(std::ceil(need_all / rw));
-      unsigned d = std::max(static_cast<unsigned>(std::ceil(need / rw)), std::min(kMinDegree, d_all));
-      d = std::clamp(d, 8u, kMaxDegree);
+      // (degrees are clamped in double: rw -> 0 as the smallest wanted value nears b)
+      const double dmax = static_cast<double>(kMaxDegree);
+      const double d_all = std::min(std::ceil(need_all / rw), dmax);
+      const double d_need = std::min(std::ceil(need / rw), dmax);
+      const unsigned d = static_cast<unsigned>(std::clamp(std::max(d_need, std::min(static_cast<double>(kMinDegree), d_all)), 8.0, dmax));
       // chunk length: re-orthonormalise before the spread of amplifications exceeds ~1e6
       // (~1e3 in FP32, whose rounding would otherwise swamp the least amplified vectors)
       const double spread = rt - rw;
-      unsigned chunk = spread > 0.0 ? static_cast<unsigned>(std::log(use32 ? 1e3 : 1e6) / spread) : d;
-      chunk = std::clamp(chunk, 4u, d);
+      const double chunk_d = spread > 0.0 ? std::log(use32 ? 1e3 : 1e6) / spread : static_cast<double>(d);
+      const unsigned chunk = static_cast<unsigned>(std::clamp(chunk_d, 4.0, static_cast<double>(d)));
       unsigned done = 0;
       if (trace_)
         std::fprintf(stderr, "refine round %u fp32 %d res %.3e degree %u rate %.4f chunk %u b %.6f worst %.6f host %.1f ms\n", round, static_cast<int>(use32), res, d, rw, chunk, b,
@@ -269,7 +279,7 @@ public:
         ctx_->check(trl_cuda_convert(h_, TRL_F32, c32, TRL_F64, cur, static_cast<std::int64_t>(blk_) * kr_), "refine narrow");
         while (done < d) {
           const unsigned L = std::min(chunk, d - done);
-          if (filter(A32_, c32, s32, L, s, c, e, top) == s32) std::swap(c32, s32);
+          if (filter(*op32_, c32, s32, L, s, c, e, top) == s32) std::swap(c32, s32);
           orthonormalize(c32);
           done += L;
         }
@@ -280,7 +290,7 @@ public:
       else {
         while (done < d) {
           const unsigned L = std::min(chunk, d - done);
-          if (filter(A_, cur, spare, L, s, c, e, top) == spare) std::swap(cur, spare); // the filtered block is in cur
+          if (filter(*op64_, cur, spare, L, s, c, e, top) == spare) std::swap(cur, spare); // the filtered block is in cur
           orthonormalize(cur);
           done += L;
         }
@@ -304,7 +314,7 @@ private:
   std::shared_ptr<Context> ctx_;
   trl_cuda_handle h_;
   const trl_csr* A_;
-  const trl_csr* A32_;
+  std::shared_ptr<const SellOp> op64_, op32_;
   trl_solve_params p_;
   unsigned kr_;
   std::int64_t n_;
@@ -346,7 +356,7 @@ private:
     double* AX = static_cast<double*>(AX_.get());
     double* T = static_cast<double*>(T_.get());
     double* C = static_cast<double*>(C_.get());
-    ctx_->check(trl_cuda_spmm_blocks(h_, A_, TRL_F64, X, AX, bs, static_cast<int>(kr_), p_.alpha, p_.beta, 0.0, nullptr), "refine Rayleigh-Ritz");
+    op64_->spmm(X, AX, static_cast<int>(kr_), p_.alpha, p_.beta);
     // lower block triangle of H: column j = X^T (op X_j), blocks k >= j
     for (unsigned j = 0; j < kr_; ++j) {
       ctx_->check(trl_cuda_block_dot(h_, TRL_F64, X, static_cast<int>(kr_), blockp(AX, j), n_, bs, C), "refine Rayleigh-Ritz");
@@ -397,22 +407,20 @@ private:
   /// point `top` (the largest kept value) so that the kept components stay O(1). X and Y are
   /// the two recurrence buffers (both overwritten); returns the one holding the result.
   template <class T>
-  T* filter(const trl_csr* A, T* X, T* Y, unsigned L, double s, double c, double e, double top)
+  T* filter(const SellOp& A, T* X, T* Y, unsigned L, double s, double c, double e, double top)
   {
-    constexpr int dt = trl::cuda::dtype_of<T>::value;
     // s * op = s*alpha*A + s*beta*I; the recurrence needs (s*op - c) / e
     const double al = s * p_.alpha, be = s * p_.beta - c;
     double sigma = e / (top - c);
     const double tau = 2.0 / sigma;
     // Y1 = (s op - c) X * sigma / e
-    ctx_->check(trl_cuda_spmm_blocks(h_, A, dt, X, Y, bs, static_cast<int>(kr_), al * sigma / e, be * sigma / e, 0.0, nullptr), "refine filter");
+    A.spmm(X, Y, static_cast<int>(kr_), al * sigma / e, be * sigma / e);
     T* prev = X;
     T* curv = Y;
     for (unsigned i = 2; i <= L; ++i) {
       const double sigma2 = 1.0 / (tau - sigma);
       // Y_{i} = 2 sigma2 / e (s op - c) Y_{i-1} - sigma sigma2 Y_{i-2}, written over Y_{i-2}
-      ctx_->check(trl_cuda_spmm_blocks(h_, A, dt, curv, prev, bs, static_cast<int>(kr_), 2.0 * sigma2 / e * al, 2.0 * sigma2 / e * be, -sigma * sigma2, prev),
-                  "refine filter");
+      A.spmm(curv, prev, static_cast<int>(kr_), 2.0 * sigma2 / e * al, 2.0 * sigma2 / e * be, -sigma * sigma2, prev);
       std::swap(prev, curv);
       sigma = sigma2;
     }
@@ -446,17 +454,24 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
   DeviceBuffer X64(ctx, sizeof(double) * static_cast<std::size_t>(n) * bs * std::max(kx, kref));
   PhaseOut out;
   double t32 = 0.0;
+  // the operator prepared for this block size (sliced-ELL copies, built on the device inside
+  // the timed solve): FP64 for the FP64 solve, the refinement and the residuals, FP32 for the
+  // FP32 phases
+  if (p.mode != TRL_MODE_FP64 && !A32) throw std::invalid_argument("FP32 and mixed modes need the FP32 copy of the operator");
+  const bool need64 = p.mode != TRL_MODE_FP32 || p.want_vectors;
+  const std::shared_ptr<const SellOp> op64 = need64 ? std::make_shared<const SellOp>(ctx, A64, static_cast<int>(bs)) : nullptr;
+  const std::shared_ptr<const SellOp> op32 = p.mode != TRL_MODE_FP64 ? std::make_shared<const SellOp>(ctx, A32, static_cast<int>(bs)) : nullptr;
+  stage("operators prepared");
 
   if (p.mode == TRL_MODE_FP64) {
-    out = run_phase_r<double, bs>(ctx, A64, p, p.max_restarts, p.tol, X0, p.want_vectors ? kx : 0, static_cast<double*>(X64.get()));
+    out = run_phase_r<double, bs>(ctx, A64, op64, p, p.max_restarts, p.tol, X0, p.want_vectors ? kx : 0, static_cast<double*>(X64.get()));
   }
   else {
-    if (!A32) throw std::invalid_argument("FP32 and mixed modes need the FP32 copy of the operator");
     DeviceBuffer X32(ctx, sizeof(float) * static_cast<std::size_t>(n) * bs * std::max(kx, kref));
     DeviceBuffer X0f(ctx, sizeof(float) * static_cast<std::size_t>(n) * bs);
     ctx->check(trl_cuda_convert(h, TRL_F32, X0f.get(), TRL_F64, X0, n * bs), "initial block");
     if (p.mode == TRL_MODE_FP32) {
-      out = run_phase_r<float, bs>(ctx, A32, p, p.max_restarts, p.tol, static_cast<const float*>(X0f.get()), kx, static_cast<float*>(X32.get()));
+      out = run_phase_r<float, bs>(ctx, A32, op32, p, p.max_restarts, p.tol, static_cast<const float*>(X0f.get()), kx, static_cast<float*>(X32.get()));
       ctx->check(trl_cuda_convert(h, TRL_F64, X64.get(), TRL_F32, X32.get(), n * bs * kx), "widen");
     }
     else {
@@ -464,7 +479,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
       trl_solve_params p32 = p;
       if (p.fp32_ncv) p32.ncv = p.fp32_ncv;
       const unsigned k32 = std::min(kref, p32.ncv / bs); // Ritz blocks the FP32 phase hands over
-      PhaseOut o32 = run_phase_r<float, bs>(ctx, A32, p32, p.max_restarts, p.fp32_tol, static_cast<const float*>(X0f.get()), k32, static_cast<float*>(X32.get()));
+      PhaseOut o32 = run_phase_r<float, bs>(ctx, A32, op32, p32, p.max_restarts, p.fp32_tol, static_cast<const float*>(X0f.get()), k32, static_cast<float*>(X32.get()));
       t32 = phase.stop();
       stage("fp32 phase done");
       info->restarts_fp32 = o32.restarts;
@@ -475,7 +490,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
       ctx->check(trl_cuda_convert(h, TRL_F64, X64.get(), TRL_F32, X32.get(), n * bs * k32), "widen");
       bool refined = false;
       if (p.refine == TRL_REFINE_CHEBYSHEV) {
-        ChebyshevRefinement<bs> cheb(ctx, A64, p.refine_fp32 ? A32 : nullptr, p, k32);
+        ChebyshevRefinement<bs> cheb(ctx, A64, op64, p.refine_fp32 ? op32 : nullptr, p, k32);
         stage("refinement buffers allocated");
         const RefineOut r = cheb.run(static_cast<double*>(X64.get()));
         stage("refinement done");
@@ -500,7 +515,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
       DeviceBuffer V0(ctx, sizeof(double) * static_cast<std::size_t>(n) * bs);
       ctx->check(trl_cuda_block_rotate(h, TRL_F64, X64.get(), static_cast<int>(kr), static_cast<const double*>(Gd.get()), 1, 1, V0.get(), n, bs), "refine start");
       ctx->check(trl_cuda_synchronize(h), "refine start");
-      out = run_phase_r<double, bs>(ctx, A64, p, p.refine_max_restarts, p.tol, static_cast<const double*>(V0.get()), p.want_vectors ? kx : 0,
+      out = run_phase_r<double, bs>(ctx, A64, op64, p, p.refine_max_restarts, p.tol, static_cast<const double*>(V0.get()), p.want_vectors ? kx : 0,
                                     static_cast<double*>(X64.get()));
       }
     }
@@ -525,7 +540,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
     std::vector<double> gh(2 * bs * bs);
     for (unsigned j = 0; j < kx; ++j) {
       const double* Xj = static_cast<const double*>(X64.get()) + static_cast<std::size_t>(j) * n * bs;
-      ctx->check(trl_cuda_spmm(h, A64, TRL_F64, Xj, R.get(), bs, p.alpha, p.beta), "residual");
+      op64->spmm(Xj, R.get(), 1, p.alpha, p.beta);
       double diag[16] = {0};
       for (unsigned c = 0; c < bs; ++c) diag[c] = (j * bs + c < p.nev) ? evals_host[j * bs + c] : 0.0;
       ctx->check(trl_cuda_mb_zero(h, static_cast<double*>(D.get()), bs), "residual");

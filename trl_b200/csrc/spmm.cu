@@ -16,54 +16,9 @@
 
 namespace {
 
+using namespace trl_detail;
+
 constexpr int kThreads = 256;
-
-template <typename T, int VEC>
-struct VecT;
-template <>
-struct VecT<double, 1> {
-  using type = double;
-};
-template <>
-struct VecT<double, 2> {
-  using type = double2;
-};
-template <>
-struct VecT<float, 1> {
-  using type = float;
-};
-template <>
-struct VecT<float, 2> {
-  using type = float2;
-};
-template <>
-struct VecT<float, 4> {
-  using type = float4;
-};
-
-template <typename T, int VEC>
-__device__ __forceinline__ void load_vec(const T* p, T (&out)[VEC])
-{
-  using V = typename VecT<T, VEC>::type;
-  const V v = __ldg(reinterpret_cast<const V*>(p));
-  if constexpr (VEC == 1) {
-    out[0] = reinterpret_cast<const T*>(&v)[0];
-  }
-  else {
-#pragma unroll
-    for (int i = 0; i < VEC; ++i) out[i] = reinterpret_cast<const T*>(&v)[i];
-  }
-}
-
-template <typename T, int VEC>
-__device__ __forceinline__ void store_vec(T* p, const T (&in)[VEC])
-{
-  using V = typename VecT<T, VEC>::type;
-  V v;
-#pragma unroll
-  for (int i = 0; i < VEC; ++i) reinterpret_cast<T*>(&v)[i] = in[i];
-  *reinterpret_cast<V*>(p) = v;
-}
 
 template <typename T, int BS>
 struct SpmmShape {
@@ -86,27 +41,6 @@ struct SpmmShape {
 // per-row walk keeps every group busy for the longest row's length, which on a Zipf row-length
 // pattern (median 21, p99 326) leaves 70% of the lane slots idle.
 constexpr int kLongRow = 32;
-
-// The CSR stream is read once: load it without allocating in L1, which keeps L1 for the
-// X rows that neighbouring rows gather again.
-__device__ __forceinline__ int ld_stream(const int32_t* p)
-{
-  int v;
-  asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ double ld_stream(const double* p)
-{
-  double v;
-  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ float ld_stream(const float* p)
-{
-  float v;
-  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-}
 
 // A warp owns RPW consecutive rows per iteration; within it a group of LPR lanes owns a row
 // and each lane VEC adjacent columns of the block.
@@ -263,7 +197,7 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
           T x[VEC];
           load_vec<T, VEC>(Xb + row * BS + sub * VEC, x);
 #pragma unroll
-          for (int i = 0; i < VEC; ++i) y[i] = alpha * acc[i] + beta * x[i];
+          for (int i = 0; i < VEC; ++i) y[i] = fma(alpha, acc[i], beta * x[i]); // explicit: the same rounding as the sliced-ELL kernel
         }
         else {
 #pragma unroll
@@ -275,7 +209,7 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
 #pragma unroll
           for (int i = 0; i < VEC; ++i) wv[i] = Wb[row * BS + sub * VEC + i];
 #pragma unroll
-          for (int i = 0; i < VEC; ++i) y[i] += gamma * wv[i];
+          for (int i = 0; i < VEC; ++i) y[i] = fma(gamma, wv[i], y[i]);
         }
         store_vec<T, VEC>(Yb + row * BS + sub * VEC, y);
       }

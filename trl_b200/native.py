@@ -62,6 +62,10 @@ CUDA_SYMBOLS = {
     "trl_cuda_spmm3": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_double, C.c_double, C.c_double, P]),
     "trl_cuda_spmm_blocks": (C.c_int, [P, P, C.c_int, P, P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, P]),
     "trl_cuda_csr_gershgorin": (C.c_int, [P, P, C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "trl_cuda_op_create": (C.c_int, [P, P, C.c_int, C.POINTER(P)]),
+    "trl_cuda_op_destroy": (C.c_int, [P, P]),
+    "trl_cuda_op_info": (C.c_int, [P, C.POINTER(I64), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "trl_cuda_op_spmm": (C.c_int, [P, P, P, P, C.c_int, C.c_double, C.c_double, C.c_double, P]),
     "trl_cuda_sddmm": (C.c_int, [P, P, P, C.c_int, P, P]),
     "trl_cuda_eigen_adjoint": (C.c_int, [P, P, P, C.c_int, P, P, C.c_double, C.c_int, P]),
     "trl_cuda_mb_copy": (C.c_int, [P, P, P, C.c_int, C.c_int]),
@@ -270,6 +274,12 @@ class Handle:
         nb, n, bs = X.shape
         self.check(self.lib.trl_cuda_spmm_blocks(self.h, C.byref(A.desc), _dtype(X), _ptr(X), _ptr(Y), bs, nb, alpha, beta, gamma, _ptr(W)))
 
+    def prepare(self, A: "DeviceCSRTensors", bs: int) -> "PreparedOp":
+        """The operator converted for repeated SpMMs with block size bs (trl_cuda_op_create)."""
+        op = P()
+        self.check(self.lib.trl_cuda_op_create(self.h, C.byref(A.desc), bs, C.byref(op)))
+        return PreparedOp(self, op, A.desc.value_dtype, bs)
+
     def csr_gershgorin(self, A: "DeviceCSRTensors", alpha: float = 1.0, beta: float = 0.0):
         lo, hi = C.c_double(0.0), C.c_double(0.0)
         self.check(self.lib.trl_cuda_csr_gershgorin(self.h, C.byref(A.desc), alpha, beta, C.byref(lo), C.byref(hi)))
@@ -321,6 +331,34 @@ class Handle:
         self.check(self.lib.trl_cuda_small_eigen(self.h, _ptr(T), nblk, bs, _ptr(beta), nev, tol, _ptr(evals), _ptr(evecs),
                                                  host.ctypes.data, C.byref(nconv)))
         return evals, evecs, host, nconv.value
+
+
+class PreparedOp:
+    """A trl_cuda_op (sliced-ELL copy of a CSR operator) owned by the handle that made it."""
+
+    def __init__(self, handle: Handle, op, dtype: int, bs: int):
+        self.handle, self.op, self.dtype, self.bs = handle, op, dtype, bs
+
+    def info(self) -> dict:
+        stored, c, longest = I64(0), C.c_int(0), C.c_int(0)
+        self.handle.check(self.handle.lib.trl_cuda_op_info(self.op, C.byref(stored), C.byref(c), C.byref(longest)))
+        return {"stored": stored.value, "slice_height": c.value, "longest_row": longest.value}
+
+    def spmm(self, X, Y, alpha: float = 1.0, beta: float = 0.0, gamma: float = 0.0, W=None):
+        """Y_j = alpha A X_j + beta X_j + gamma W_j; X, Y, W of shape (n, bs) or (nb, n, bs)."""
+        nb = 1 if X.dim() == 2 else X.shape[0]
+        self.handle.check(self.handle.lib.trl_cuda_op_spmm(self.handle.h, self.op, _ptr(X), _ptr(Y), nb, alpha, beta, gamma, _ptr(W)))
+
+    def close(self):
+        if self.op and getattr(self.handle, "h", None):
+            self.handle.lib.trl_cuda_op_destroy(self.handle.h, self.op)
+        self.op = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass
