@@ -267,13 +267,14 @@ constexpr int kSpmmThreads = 256;
 constexpr int kSpmmWarps = kSpmmThreads / 32;
 
 // Per instantiation: NBG blocks accumulated per pass over a slice (1 for the single-block
-// SpMM; the multi-block SpMM re-reads a slice's indices and values for each group of NBG
-// blocks), UG slots per group, and the CTAs per SM the registers must allow.
+// SpMM; the multi-block SpMM takes two blocks per pass and re-reads a slice's indices and
+// values, from L2, for each pair), UG slots per group, and the CTAs per SM the registers
+// must allow.
 template <typename T, int BS, int NBG>
 struct SellTune {
   static constexpr int lane_bytes = SellShape<T, BS>::VEC * static_cast<int>(sizeof(T));
-  static constexpr int ug = (NBG == 1 ? 64 : 32) / lane_bytes;
-  static constexpr int UG = ug < 1 ? 1 : (ug > 4 ? 4 : ug);
+  static constexpr int ug = 64 / lane_bytes;
+  static constexpr int UG = NBG == 1 ? (ug > 4 ? 4 : ug) : 2;
   static constexpr int MINB = NBG == 1 ? 4 : 2;
 };
 
@@ -587,7 +588,7 @@ int trl_cuda_op_spmm(trl_cuda_handle h, trl_cuda_op op, const void* X, void* Y, 
                                                    static_cast<const T*>(X), static_cast<T*>(Y), static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma),
                                                    static_cast<const T*>(W), nb, op->n * BS);
     };
-    if (nb > 1) launch(k_spmm_sell<T, BS, 4>, SellTune<T, BS, 4>::MINB);
+    if (nb > 1) launch(k_spmm_sell<T, BS, 2>, SellTune<T, BS, 2>::MINB);
     else launch(k_spmm_sell<T, BS, 1>, SellTune<T, BS, 1>::MINB);
     st = after_launch(h, "spmm (sliced ELL)");
   }));
