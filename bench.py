@@ -63,7 +63,7 @@ def make_workload(name: str):
         return A, -1.0, sigma, (f"elasticity27 64^3 nodes x 3 dofs n={A.n} nnz={A.nnz} (boundary-trimmed), 64 smallest via sigma*I - A, "
                                 f"sigma = Gershgorin bound {sigma:.6f}, bs=8 ncv=384 tol=1e-10")
     if name == "zipf4m":
-        A = P.zipf_symmetric(4_194_304, alpha=1.5, cap=512, seed=42)
+        A = P.zipf_symmetric(int(os.environ.get("TRL_BENCH_ZIPF_N", 4_194_304)), alpha=1.5, cap=512, seed=42)
         return A, 1.0, 0.0, f"zipf_symmetric n={A.n} nnz={A.nnz} (Zipf(1.5) degrees capped at 512, mirrored), 100 largest |lambda|, ncv=32*bs, tol=1e-10"
     raise ValueError(name)
 
@@ -569,6 +569,7 @@ def profile_case(args):
                  one JSON line each (restarts, applies, refinement rounds, residuals, seconds);
     spmm         the prepared operator's SpMM, --reps launches (--nb blocks, --fp32);
     spmm-csr     the CSR kernel (trl_cuda_spmm / _blocks) on the same operands;
+                 (fp64-fullreorth, fp64-cgs2: FP64 with every step projected);
     spmm-rates   prepared operator against the CSR kernel, one JSON line per dtype and block
                  count, each timed launch behind an L2 flush;
     dot / update one multi-block inner product / projection update against --nblk blocks;
@@ -597,14 +598,16 @@ def profile_case(args):
             S.solve(native.TRL_MODE_MIXED)
         else:
             modes = {"fp64": (native.TRL_MODE_FP64, {}), "fp32": (native.TRL_MODE_FP32, {}), "mixed": (native.TRL_MODE_MIXED, {}),
-                     "mixed-lanczos": (native.TRL_MODE_MIXED, {"refine": native.TRL_REFINE_LANCZOS})}
+                     "mixed-lanczos": (native.TRL_MODE_MIXED, {"refine": native.TRL_REFINE_LANCZOS}),
+                     "fp64-fullreorth": (native.TRL_MODE_FP64, {"reorth": native.TRL_REORTH_CGS_IFNEEDED}),
+                     "fp64-cgs2": (native.TRL_MODE_FP64, {"reorth": native.TRL_REORTH_CGS2})}
             for name in args.modes.split(","):
                 mode, kw = modes[name]
-                ms, outs, _, launches = S.timed(mode, 1, max_restarts=args.restarts, refine_max_restarts=args.restarts, **kw)
+                ms, outs, _, launches = S.timed(mode, 1, max_restarts=args.restarts, refine_max_restarts=args.restarts, **dict(kw, **json.loads(args.params)))
                 o = outs[-1]
                 keep = ("converged", "restarts", "n_op_apply", "restarts_fp32", "n_op_apply_fp32", "seconds_fp32", "refine_rounds", "refine_degree",
                         "refine_degree_fp32", "max_rel_residual", "max_theta_residual")
-                print(json.dumps({"case": "solves", "workload": args.workload, "bs": bs, "mode": name, "seconds": ms / 1e3, "launches": launches,
+                print(json.dumps({"case": "solves", "workload": args.workload, "bs": bs, "mode": name, "params": json.loads(args.params), "seconds": ms / 1e3, "launches": launches,
                                   **{k: o[k] for k in keep}, "evals_head": [float(x) for x in o["evals"][:3]],
                                   "evals_tail": [float(x) for x in o["evals"][-3:]]}), flush=True)
     elif args.case == "spmm-rates":
@@ -717,6 +720,7 @@ def main():
                     default=None, help="profiling driver: run one piece of a workload and exit (see profile_case)")
     ap.add_argument("--workload", default="aniso96", choices=["aniso96", "elast64", "zipf4m"])
     ap.add_argument("--modes", default="fp64,mixed")
+    ap.add_argument("--params", default="{}", help="solves: extra solver parameters (JSON object of trl_solve_params fields)")
     ap.add_argument("--bs", type=int, default=8)
     ap.add_argument("--nb", type=int, default=1)
     ap.add_argument("--restarts", type=int, default=3)

@@ -45,6 +45,15 @@
 
 namespace trl::cuda {
 
+/// Device allocation failed (TRL_ENOMEM); a std::runtime_error, as the reference's errors.
+struct out_of_device_memory : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+/// A bounded device-side wait gave up (TRL_ETIMEOUT).
+struct device_timeout : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 template <class T>
 struct dtype_of;
 template <>
@@ -99,6 +108,8 @@ public:
     case TRL_ENOTSUP: throw std::invalid_argument(msg);
     case TRL_ECHOLESKY: throw std::runtime_error("Cholesky factorization failed in orthonormalize");
     case TRL_EEIGEN: throw std::runtime_error("Eigendecomposition failed");
+    case TRL_ENOMEM: throw out_of_device_memory(msg);
+    case TRL_ETIMEOUT: throw device_timeout(msg);
     default: throw std::runtime_error(msg);
     }
   }

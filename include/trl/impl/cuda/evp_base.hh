@@ -15,6 +15,9 @@
 #include "multivector.hh"
 
 #include <cassert>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
@@ -98,9 +101,70 @@ public:
       ctx_->check(trl_cuda_small_eigen_partial(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
                                                static_cast<int>(kvec), static_cast<double*>(evals_dev_.get()), eigenvectors->data(), eigenvalues.data(), &nconv),
                   "solve_small_dense");
+#ifdef TRL_DEBUG_TRACE
+      debug_compare_small(B, beta, nev, kvec, nconv);
+#endif
     }
     return static_cast<std::size_t>(nconv);
   }
+
+#ifdef TRL_DEBUG_TRACE
+  /// Debug builds with TRL_DUMP_SMALL=<dir>: every projected problem is solved again by the
+  /// full eigensolver; when the kept eigenvectors disagree (per column, up to sign) the
+  /// matrix, beta and both results are written to <dir>.
+  void debug_compare_small(const BlockMatrix& B, BlockMatrixBlockView beta, std::size_t nev, std::size_t kvec, int nconv)
+  {
+    static const char* dir = std::getenv("TRL_DUMP_SMALL");
+    static int call = 0;
+    if (!dir) return;
+    ++call;
+    const std::size_t nblk = B.block_rows(), N = nblk * blocksize, NN = N * N;
+    DeviceBuffer Yf(ctx_, sizeof(double) * NN), ev(ctx_, sizeof(double) * N);
+    std::vector<double> evh(N), yp(NN), yf(NN), Th(NN), bh(blocksize * blocksize);
+    int nc2 = 0;
+    ctx_->check(trl_cuda_small_eigen(ctx_->handle(), B.data(), static_cast<int>(nblk), blocksize, beta.data_, static_cast<int>(nev), tolerance_,
+                                     static_cast<double*>(ev.get()), static_cast<double*>(Yf.get()), evh.data(), &nc2), "debug");
+    ctx_->check(trl_cuda_memcpy(ctx_->handle(), yp.data(), eigenvectors->data(), sizeof(double) * NN, TRL_D2H), "debug");
+    ctx_->check(trl_cuda_memcpy(ctx_->handle(), yf.data(), Yf.get(), sizeof(double) * NN, TRL_D2H), "debug");
+    ctx_->check(trl_cuda_memcpy(ctx_->handle(), Th.data(), B.data(), sizeof(double) * NN, TRL_D2H), "debug");
+    ctx_->check(trl_cuda_memcpy(ctx_->handle(), bh.data(), beta.data_, sizeof(double) * blocksize * blocksize, TRL_D2H), "debug");
+    auto at = [&](const std::vector<double>& Y, std::size_t r, std::size_t c) { // block layout
+      return Y[((r / blocksize) * nblk + c / blocksize) * blocksize * blocksize + (r % blocksize) * blocksize + c % blocksize];
+    };
+    double worst_ev = 0.0, worst_vec = 0.0;
+    std::size_t worst_col = 0;
+    for (std::size_t c = 0; c < N; ++c) worst_ev = std::max(worst_ev, std::abs(evh[c] - eigenvalues[c]));
+    for (std::size_t c = 0; c < kvec; ++c) {
+      double dp = 0.0, dm = 0.0;
+      for (std::size_t r = 0; r < N; ++r) {
+        dp = std::max(dp, std::abs(at(yp, r, c) - at(yf, r, c)));
+        dm = std::max(dm, std::abs(at(yp, r, c) + at(yf, r, c)));
+      }
+      if (std::min(dp, dm) > worst_vec) {
+        worst_vec = std::min(dp, dm);
+        worst_col = c;
+      }
+    }
+    std::fprintf(stderr, "small %d N %zu nconv %d/%d ev_diff %.3e vec_diff %.3e col %zu top %.12f %.12f\n", call, N, nconv, nc2, worst_ev, worst_vec, worst_col,
+                 eigenvalues[0], eigenvalues[1]);
+    static const double dump_above = std::getenv("TRL_DUMP_ABOVE") ? std::atof(std::getenv("TRL_DUMP_ABOVE")) : 1e300;
+    static int dumped = 0;
+    if (worst_vec > 1e-6 || nconv != nc2 || (std::abs(eigenvalues[0]) > dump_above && dumped++ < 2) || (call >= 1 && std::getenv("TRL_DUMP_ALL"))) {
+      const std::string base = std::string(dir) + "/small_" + std::to_string(call);
+      if (FILE* f = std::fopen((base + ".bin").c_str(), "wb")) {
+        const std::int64_t hdr[4] = {static_cast<std::int64_t>(nblk), blocksize, static_cast<std::int64_t>(kvec), static_cast<std::int64_t>(nev)};
+        std::fwrite(hdr, sizeof hdr, 1, f);
+        std::fwrite(Th.data(), sizeof(double), NN, f);
+        std::fwrite(bh.data(), sizeof(double), bh.size(), f);
+        std::fwrite(eigenvalues.data(), sizeof(double), N, f);
+        std::fwrite(yp.data(), sizeof(double), NN, f);
+        std::fwrite(evh.data(), sizeof(double), N, f);
+        std::fwrite(yf.data(), sizeof(double), NN, f);
+        std::fclose(f);
+      }
+    }
+  }
+#endif
 
   const std::vector<Scalar>& get_current_eigenvalues() const { return eigenvalues; }
 

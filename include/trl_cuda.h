@@ -76,6 +76,16 @@ const char* trl_cuda_status_string(int status);
 /* Number of kernels this handle has launched (diagnostics; counts every launch). */
 uint64_t trl_cuda_launch_count(trl_cuda_handle handle);
 
+/* ---- failure injection (tests of the error paths; no counterpart in the reference) -------
+ * trl_cuda_inject_alloc_failures: the handle's next `count` calls of trl_cuda_malloc fail with
+ * TRL_ENOMEM (the device is not touched); 0 clears. trl_cuda_test_bounded_wait: enqueues a
+ * kernel whose wait on a shared-memory barrier can never complete; the wait gives up after
+ * `polls` polls (at most 2^24), the kernel returns, and the next
+ * trl_cuda_synchronize reports TRL_ETIMEOUT, as every bounded device wait of this library
+ * does. The handle stays usable. */
+int trl_cuda_inject_alloc_failures(trl_cuda_handle handle, int count);
+int trl_cuda_test_bounded_wait(trl_cuda_handle handle, unsigned polls);
+
 /* ---- per-kernel-class device timing ---------------------------------------------------
  * When enabled, every outermost C-ABI call is bracketed by CUDA events on the handle's
  * stream and credited with its algorithmic bytes (data each operand must move once) and
@@ -158,7 +168,8 @@ int trl_cuda_block_dot(trl_cuda_handle h, int dtype, const void* V, int nblk, co
  * the device current); make that first call before any stream capture. All calls share the
  * one array: calls that may run at the same time on the GPU (different streams, or several
  * threads) race on it and must be serialised by the caller. The array's contents left by a
- * previous call are never read.
+ * previous call are never read. The looked-up address is kept for the life of the process:
+ * after cudaDeviceReset on a device this entry point is no longer valid on that device.
  * Returns TRL_OK, TRL_EINVAL, TRL_ENOTSUP or TRL_ECUDA (no error message is recorded). */
 #define TRL_CUDA_NOALLOC_MAX_ENTRIES 16384
 int trl_cuda_block_dot_noalloc(void* stream, int dtype, const void* V, int nblk, const void* W, int64_t n, int bs, double* C);

@@ -452,6 +452,27 @@ def _partial_cases():
         T[kr * bs:(kr + 1) * bs, : kr * bs] = C
         T[: kr * bs, kr * bs:(kr + 1) * bs] = C.T
         cases.append((f"restart{N}", T, bs) + ((nev,) if nev else ()))
+    # kept Ritz values on both sides of zero whose couplings to the next block are ~1e-160
+    # (fully converged pairs): the squares of those entries underflow, and a Householder
+    # reflector built from their norm is not orthogonal unless they are treated as zero (the
+    # shape of the 524,288-row Zipf solve at block size 8)
+    bs, nblk, kr = 8, 32, 13
+    N = nblk * bs
+    T = np.zeros((N, N))
+    kept = np.concatenate([rng.uniform(26.0, 27.0, kr * bs // 2), -rng.uniform(26.0, 27.0, kr * bs - kr * bs // 2)])
+    T[: kr * bs, : kr * bs] = np.diag(kept[np.argsort(-np.abs(kept))])
+    for b in range(kr, nblk):
+        D = rng.standard_normal((bs, bs)) * 5
+        T[b * bs:(b + 1) * bs, b * bs:(b + 1) * bs] = D + D.T
+        if b + 1 < nblk:
+            Bt = np.triu(rng.standard_normal((bs, bs))) * 8
+            T[(b + 1) * bs:(b + 2) * bs, b * bs:(b + 1) * bs] = Bt
+            T[b * bs:(b + 1) * bs, (b + 1) * bs:(b + 2) * bs] = Bt.T
+    C = rng.standard_normal((bs, kr * bs)) * 1e-4
+    C[:, :4] *= 1e-156
+    T[kr * bs:(kr + 1) * bs, : kr * bs] = C
+    T[: kr * bs, kr * bs:(kr + 1) * bs] = C.T
+    cases.append(("restart_tiny_coupling256", T, bs, 100))
     return cases
 
 

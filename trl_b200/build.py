@@ -5,7 +5,8 @@ travel with the source tree to the GPU host):
 * ``libtrl_cuda.so``       the sm_100a kernels behind the C ABI (include/trl_cuda.h);
 * ``libtrl_solver.so``     trl's BlockLanczos driver, unchanged, on the CUDA backend
                            (include/trl_solver.h) — compiled against the reference headers;
-* ``trl_cuda_ref_tests``   the reference's own test bodies on the CUDA backend.
+* ``trl_cuda_ref_tests``   the reference's own test bodies on the CUDA backend (a test
+                           program; source in tests/host/).
 
 The last two need the reference checkout (trl is header-only); without it only
 ``libtrl_cuda.so`` is built.
@@ -29,6 +30,10 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["context.cu", "blockvec.cu", "spmm.cu", "sell.cu", "small.cu"]
+# TRL_DEBUG_TRACE=1 at build time compiles the stderr traces of the partial
+# reorthogonalisation and of the mixed-mode refinement in (enabled at run time by
+# TRL_PARTIAL_TRACE / TRL_REFINE_TRACE); rebuild from scratch after changing it
+DEBUG = ["-DTRL_DEBUG_TRACE"] if os.environ.get("TRL_DEBUG_TRACE") else []
 # the header-only reference checkout (build time only): $TRL_REFERENCE or the default mount
 DEFAULT_REF = os.environ.get("TRL_REFERENCE", "/root/reference")
 
@@ -66,7 +71,7 @@ def build_cuda(verbose: bool = False, jobs: int = 8) -> str:
         o = os.path.join(OBJ, src.replace(".cu", ".o"))
         objs.append(o)
         if _newer(o, [s] + hdrs):
-            cmds.append([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", "-c", s, "-o", o])
+            cmds.append([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", *DEBUG, f"-I{INCLUDE}", "-c", s, "-o", o])
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         list(ex.map(lambda c: _run(c, verbose), cmds))
     so = os.path.join(LIB, "libtrl_cuda.so")
@@ -81,7 +86,7 @@ def build_solver(ref: str = DEFAULT_REF, verbose: bool = False) -> list[str]:
     if not os.path.isdir(ref_inc):
         return []
     hdrs = _headers(INCLUDE) + _headers(ref_inc)
-    common = [CXX, "-std=c++20", "-O2", "-fPIC", f"-I{INCLUDE}", f"-I{ref_inc}", f"-I{CUDA_HOME}/include"]
+    common = [CXX, "-std=c++20", "-O2", "-fPIC", *DEBUG, f"-I{INCLUDE}", f"-I{ref_inc}", f"-I{CUDA_HOME}/include"]
     link = [f"-L{LIB}", "-ltrl_cuda", f"-L{CUDA_HOME}/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{CUDA_HOME}/lib64"]
     out = []
     srcs = [os.path.join(CSRC, "solver", f) for f in ("solver_capi.cc", "mtx.cc")]
@@ -89,7 +94,7 @@ def build_solver(ref: str = DEFAULT_REF, verbose: bool = False) -> list[str]:
     if _newer(so, srcs + [os.path.join(LIB, "libtrl_cuda.so")] + hdrs):
         _run(common + ["-shared", "-o", so, *srcs] + link + ["-pthread"], verbose)
     out.append(so)
-    src = os.path.join(CSRC, "solver", "ref_tests_cuda.cc")
+    src = os.path.join(ROOT, "tests", "host", "ref_tests_cuda.cc")  # a test program
     exe = os.path.join(LIB, "trl_cuda_ref_tests")
     if os.path.isdir(ref_tests) and _newer(exe, [src, os.path.join(LIB, "libtrl_cuda.so")] + hdrs + _headers(ref_tests)):
         _run(common + [f"-I{ref_tests}", "-o", exe, src] + link, verbose)

@@ -1403,7 +1403,9 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
     if (st) return st;
     k_select_block3<<<1, 256, 0, h->stream>>>(flag1, flag2, Gw0, Gw1, Gw2, G, BB);
     st = after_launch(h, "select");
-    // TRL_PARTIAL_TRACE: one stderr line per call (synchronises; diagnostics only)
+#ifdef TRL_DEBUG_TRACE
+    // debug builds (-DTRL_DEBUG_TRACE) with TRL_PARTIAL_TRACE set: one stderr line per call
+    // (synchronises; diagnostics only)
     static const bool trace = std::getenv("TRL_PARTIAL_TRACE") != nullptr;
     if (!st && trace) {
       double eg[2 * 256];
@@ -1416,6 +1418,7 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
       for (int c = 0; c < bs; ++c) tr += eg[BB + c * bs + c];
       std::fprintf(stderr, "partial nblk %d loss %.3e projected %d forced %d second %d\n", nblk, std::sqrt(e2 / tr), fl[0] & 1, (fl[0] >> 1) & 1, fl[1]);
     }
+#endif
   }));
   return st;
 }

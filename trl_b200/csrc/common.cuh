@@ -34,6 +34,7 @@ struct trl_cuda_context {
   void* syevd_work = nullptr;
   size_t syevd_work_bytes = 0;
   uint64_t launches = 0;
+  int refuse_allocs = 0; // trl_cuda_inject_alloc_failures: allocations still to refuse
   std::string last_error;
   // per-kernel-class device timing (trl_cuda_profile_*)
   bool profiling = false;

@@ -269,6 +269,10 @@ int trl_cuda_malloc(trl_cuda_handle h, void** ptr, size_t bytes)
   if (!ptr) return set_error(h, TRL_EINVAL, "null output pointer");
   *ptr = nullptr;
   if (bytes == 0) return TRL_OK;
+  if (h->refuse_allocs > 0) {
+    --h->refuse_allocs;
+    return set_error(h, TRL_ENOMEM, "allocation of %zu bytes refused (injected failure)", bytes);
+  }
   if (!h->pool) {
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
@@ -332,3 +336,34 @@ int trl_cuda_memset_zero(trl_cuda_handle h, void* ptr, size_t bytes)
 }
 
 } // extern "C"
+
+namespace {
+
+// One thread waits on a shared-memory mbarrier that expects two arrivals and gets one: the
+// phase never completes, the wait gives up after `polls` polls and records TRL_DEV_TIMEOUT.
+__global__ void k_wait_never_completes(int* status, unsigned polls)
+{
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 2);
+  mbar_arrive(&bar);
+  mbar_wait(&bar, 0, status, polls);
+}
+
+} // namespace
+
+extern "C" int trl_cuda_inject_alloc_failures(trl_cuda_handle h, int count)
+{
+  TRL_CHECK_HANDLE(h);
+  if (count < 0) return set_error(h, TRL_EINVAL, "negative count");
+  h->refuse_allocs = count;
+  return TRL_OK;
+}
+
+extern "C" int trl_cuda_test_bounded_wait(trl_cuda_handle h, unsigned polls)
+{
+  TRL_CHECK_HANDLE(h);
+  if (polls == 0 || polls > (1u << 24)) return set_error(h, TRL_EINVAL, "polls must be in [1, 2^24]");
+  k_wait_never_completes<<<1, 32, 0, h->stream>>>(h->d_status, polls);
+  return after_launch(h, "bounded wait");
+}

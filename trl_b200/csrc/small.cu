@@ -45,16 +45,42 @@ __global__ void k_mb_set_diag(double* __restrict__ dst, DiagValues d, int bs)
   if (i < bs) dst[i * bs + i] = d.v[i];
 }
 
+// max |T_ij| over the block matrix (one CTA) into *out
+__global__ void __launch_bounds__(1024) k_max_abs(const double* __restrict__ T, int64_t count, double* __restrict__ out)
+{
+  __shared__ double red[32];
+  double m = 0.0;
+  for (int64_t e = threadIdx.x; e < count; e += blockDim.x) m = fmax(m, fabs(T[e]));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) *out = m;
+  }
+}
+
+// Entries below kFlushRel * max|T| are set to zero when the dense copy is assembled: they
+// change no eigenvalue by more than N * 1e-30 * ||T||, far below rounding, while leaving
+// them in lets their squares underflow inside the Householder reduction (a converged Ritz
+// pair's coupling in a thick-restart matrix can be ~1e-160 next to entries of order 10);
+// a reflector built from an underflowed norm is not orthogonal, and the computed spectrum is
+// then wrong (cuSOLVER's syevd on the GPU fails the same way on such matrices).
+constexpr double kFlushRel = 1e-30;
+
 // dense column-major A (N x N) from the lower triangle of the block matrix T
-__global__ void k_assemble_dense(const double* __restrict__ T, int nblk, int bs, double* __restrict__ A)
+__global__ void k_assemble_dense(const double* __restrict__ T, int nblk, int bs, const double* __restrict__ tmax, double* __restrict__ A)
 {
   const int N = nblk * bs;
   const int64_t total = static_cast<int64_t>(N) * N;
+  const double floor = kFlushRel * *tmax;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int c = static_cast<int>(e / N), r = static_cast<int>(e % N); // A[c*N + r] = M(r, c)
     const int hi = r > c ? r : c, lo = r > c ? c : r;
     const int bi = hi / bs, ri = hi % bs, bj = lo / bs, cj = lo % bs;
-    A[e] = T[(static_cast<int64_t>(bi) * nblk + bj) * bs * bs + ri * bs + cj];
+    const double v = T[(static_cast<int64_t>(bi) * nblk + bj) * bs * bs + ri * bs + cj];
+    A[e] = fabs(v) < floor ? 0.0 : v;
   }
 }
 
@@ -202,7 +228,8 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
   const size_t off_w = a_bytes;
   const size_t off_perm = off_w + w_bytes;
   const size_t off_info = off_perm + sizeof(int) * N + 64;
-  const size_t total = off_info + 64;
+  const size_t off_tmax = (off_info + 64 + 15) / 16 * 16; // a double: 8-byte aligned whatever N is
+  const size_t total = off_tmax + 64;
   char* ws = static_cast<char*>(workspace(h, total));
   if (!ws) return TRL_ENOMEM;
   double* A = reinterpret_cast<double*>(ws);
@@ -210,6 +237,7 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
   int* perm = reinterpret_cast<int*>(ws + off_perm);
   int* info = reinterpret_cast<int*>(ws + off_info);
   int* count = info + 1;
+  double* tmax = reinterpret_cast<double*>(ws + off_tmax);
 
   int lwork = 0;
   cs = cusolverDnDsyevd_bufferSize(sh, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, A, N, w, &lwork);
@@ -228,7 +256,8 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
   }
 
   const unsigned g = grid_for(h, static_cast<int64_t>(N) * N, 256, 4);
-  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, A);
+  k_max_abs<<<1, 1024, 0, h->stream>>>(T, static_cast<int64_t>(N) * N, tmax);
+  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, tmax, A);
   if (int st = after_launch(h, "assemble")) return st;
   cs = cusolverDnDsyevd(sh, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, A, N, w, static_cast<double*>(h->syevd_work), lwork, info);
   if (cs != CUSOLVER_STATUS_SUCCESS) return set_error(h, TRL_ECUDA, "syevd failed (%d)", static_cast<int>(cs));
@@ -290,6 +319,7 @@ namespace {
 //   N <= kTriMaxN      16 CTAs, rows in global memory.
 // Rows per CTA * N * 8 B must fit one CTA's shared memory (227 KB) for the first two.
 constexpr int kTriThreads = 512;
+constexpr double kTinyNorm2 = 1e-290; // squared column norms below this are treated as zero
 constexpr int kTriMaxN8 = 448;
 constexpr int kTriMaxN16 = 640;
 constexpr int kTriMaxN = 1024;
@@ -427,7 +457,9 @@ __global__ void __launch_bounds__(kTriThreads, 1)
     const double xnorm2 = local_sum(part);
     const double x0 = part[NP];
     double tau = 0.0, beta = x0, scale = 0.0;
-    if (xnorm2 > 0.0) {
+    // a column whose squares underflow is left as it is (H = I): a reflector built from a
+    // norm computed in the subnormal range would not be orthogonal
+    if (xnorm2 > 0.0 && x0 * x0 + xnorm2 > kTinyNorm2) {
       beta = -copysign(sqrt(x0 * x0 + xnorm2), x0);
       tau = (beta - x0) / beta;
       scale = 1.0 / (x0 - beta);
@@ -964,7 +996,7 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   const size_t nchunks = static_cast<size_t>(N - 2 + kWyRows - 1) / kWyRows;
   const size_t doubles = 2 * NN + 4 * static_cast<size_t>(N) + (2 + kFactorRows) * NK + nchunks * kWyRows * kWyRows;
   const size_t ints = 3 * static_cast<size_t>(N) + 8;
-  char* ws = static_cast<char*>(workspace(h, sizeof(double) * doubles + sizeof(int) * ints + 256));
+  char* ws = static_cast<char*>(workspace(h, sizeof(double) * (doubles + 1) + sizeof(int) * ints + 256));
   if (!ws) return TRL_ENOMEM;
   double* A = reinterpret_cast<double*>(ws);
   double* refl = A + NN;
@@ -980,9 +1012,11 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   int* sel = perm + N;
   int* slot = sel + N;
   int* flags = slot + N; // [0] = 0 (no solver error), [1] = converged count
+  double* tmax = reinterpret_cast<double*>(ws + (sizeof(double) * doubles + sizeof(int) * ints + 15) / 16 * 16);
 
   const unsigned g = grid_for(h, static_cast<int64_t>(N) * N, 256, 4);
-  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, A);
+  k_max_abs<<<1, 1024, 0, h->stream>>>(T, static_cast<int64_t>(N) * N, tmax);
+  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, tmax, A);
   if (int st = after_launch(h, "assemble")) return st;
   cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream);
   {

@@ -320,7 +320,11 @@ private:
   std::int64_t n_;
   std::size_t blk_;
   DeviceBuffer Y_, AX_, AXr_, R_, T_, C_, Z_, ev_, small_, X32_, Y32_;
-  const bool trace_ = std::getenv("TRL_REFINE_TRACE") != nullptr; // per-round log on stderr
+#ifdef TRL_DEBUG_TRACE
+  const bool trace_ = std::getenv("TRL_REFINE_TRACE") != nullptr; // debug builds: per-round log on stderr
+#else
+  static constexpr bool trace_ = false;
+#endif
   const std::chrono::steady_clock::time_point t0_ = std::chrono::steady_clock::now();
 
   template <class T>
@@ -445,8 +449,12 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
 
   EventTimer total(stream), phase(stream);
   total.start();
-  // TRL_REFINE_TRACE: host timestamps of the solve's stages on stderr
+#ifdef TRL_DEBUG_TRACE
+  // debug builds with TRL_REFINE_TRACE set: host timestamps of the solve's stages on stderr
   const bool trace = std::getenv("TRL_REFINE_TRACE") != nullptr;
+#else
+  constexpr bool trace = false;
+#endif
   const auto host0 = std::chrono::steady_clock::now();
   const auto stage = [&](const char* what) {
     if (trace) std::fprintf(stderr, "solve %s host %.1f ms\n", what, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count());
@@ -677,6 +685,12 @@ int trl_solve_csr_device(trl_cuda_handle h, const trl_solve_params* p, const trl
   catch (const std::invalid_argument& e) {
     return fail(e, TRL_EINVAL);
   }
+  catch (const trl::cuda::out_of_device_memory& e) {
+    return fail(e, TRL_ENOMEM);
+  }
+  catch (const trl::cuda::device_timeout& e) {
+    return fail(e, TRL_ETIMEOUT);
+  }
   catch (const std::exception& e) {
     const std::string w = e.what();
     return fail(e, w.find("Cholesky") != std::string::npos ? TRL_ECHOLESKY : (w.find("Eigendecomposition") != std::string::npos ? TRL_EEIGEN : TRL_ECUDA));
@@ -728,6 +742,14 @@ int trl_solve_csr_host(const trl_solve_params* p, int device, int64_t n, int64_t
   catch (const std::invalid_argument& e) {
     if (hc && lock.owns_lock()) hc->ctx.reset(); // a failed call may leave recorded work behind: start afresh
     return fail(e, TRL_EINVAL);
+  }
+  catch (const trl::cuda::out_of_device_memory& e) {
+    if (hc && lock.owns_lock()) hc->ctx.reset();
+    return fail(e, TRL_ENOMEM);
+  }
+  catch (const trl::cuda::device_timeout& e) {
+    if (hc && lock.owns_lock()) hc->ctx.reset();
+    return fail(e, TRL_ETIMEOUT);
   }
   catch (const std::exception& e) {
     if (hc && lock.owns_lock()) hc->ctx.reset();

@@ -39,6 +39,8 @@ CUDA_SYMBOLS = {
     "trl_cuda_last_error": (C.c_char_p, [P]),
     "trl_cuda_status_string": (C.c_char_p, [C.c_int]),
     "trl_cuda_launch_count": (C.c_uint64, [P]),
+    "trl_cuda_inject_alloc_failures": (C.c_int, [P, C.c_int]),
+    "trl_cuda_test_bounded_wait": (C.c_int, [P, C.c_uint]),
     "trl_cuda_malloc": (C.c_int, [P, C.POINTER(P), C.c_size_t]),
     "trl_cuda_free": (C.c_int, [P, P]),
     "trl_cuda_memcpy": (C.c_int, [P, P, P, C.c_size_t, C.c_int]),
