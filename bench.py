@@ -68,6 +68,8 @@ def make_workload(name: str):
     raise ValueError(name)
 
 
+REFINE_NAMES = {0: "lanczos", 1: "chebyshev", 2: "auto"}
+
 # solve shapes of the secondary workloads: (bs, nev, ncv)
 SHAPES = {"elast64": [(8, 64, 384)], "zipf4m": [(4, 100, 128), (8, 100, 256), (16, 100, 512)]}
 
@@ -360,8 +362,8 @@ def secondary(h, name: str, modes: list[str]) -> list[dict]:
         row = {"workload": name, "desc": desc, "bs": bs, "nev": nev, "ncv": ncv, "n": A.n, "nnz": A.nnz, "generate_s": gen_s}
         evs = {}
         for mode in modes:
-            m = {"fp64": native.TRL_MODE_FP64, "mixed": native.TRL_MODE_MIXED, "mixed-lanczos": native.TRL_MODE_MIXED}[mode]
-            kw = {"refine": native.TRL_REFINE_LANCZOS} if mode == "mixed-lanczos" else {}
+            m = {"fp64": native.TRL_MODE_FP64, "mixed": native.TRL_MODE_MIXED, "mixed-lanczos": native.TRL_MODE_MIXED, "mixed-chebyshev": native.TRL_MODE_MIXED}[mode]
+            kw = {"mixed-lanczos": {"refine": native.TRL_REFINE_LANCZOS}, "mixed-chebyshev": {"refine": native.TRL_REFINE_CHEBYSHEV}}.get(mode, {})
             ms, outs, _, launches = S.timed(m, 1, **kw)
             o = outs[-1]
             evs[mode] = o["evals"]
@@ -369,6 +371,8 @@ def secondary(h, name: str, modes: list[str]) -> list[dict]:
                  "max_rel_residual": o["max_rel_residual"], "max_theta_residual": o["max_theta_residual"], "kernel_launches": launches}
             if m == native.TRL_MODE_MIXED:
                 r.update(restarts_fp32=o["restarts_fp32"], n_op_apply_fp32=o["n_op_apply_fp32"], seconds_fp32_phase=o["seconds_fp32"],
+                         refine_used=REFINE_NAMES.get(o["refine_used"]), refine_predicted_chebyshev_s=o["refine_predicted_s"],
+                         refine_estimated_lanczos_s=o["refine_lanczos_estimate_s"],
                          refine_rounds=o["refine_rounds"], refine_degree=o["refine_degree"], refine_degree_fp32=o["refine_degree_fp32"])
             row[mode] = r
         if "fp64" in evs:
@@ -531,7 +535,9 @@ def trl_arm(args, world, rank, local):
                      "max_rel_residual": o64["max_rel_residual"], "max_rel_err_vs_analytic": rel_err(o64["evals"], exact),
                      "max_rel_err_vs_reference": rel_err(o64["evals"], ref_evals)},
             "mixed": {"seconds": msmx / 1e3, "speedup_vs_fp64": ms64 / msmx,
-                      "refine": "Chebyshev-filtered subspace iteration + Rayleigh-Ritz on nev/bs+2 blocks (FP32 filter rounds, then FP64)",
+                      "refine": "automatic: Chebyshev-filtered subspace iteration + Rayleigh-Ritz on nev/bs+2 blocks when predicted faster than a BlockLanczos restart from the FP32 Ritz vectors",
+                      "refine_used": REFINE_NAMES.get(omx["refine_used"]), "refine_predicted_chebyshev_s": omx["refine_predicted_s"],
+                      "refine_estimated_lanczos_s": omx["refine_lanczos_estimate_s"],
                       "restarts_fp32": omx["restarts_fp32"], "n_op_apply_fp32": omx["n_op_apply_fp32"], "seconds_fp32_phase": omx["seconds_fp32"],
                       "refine_rounds": omx["refine_rounds"], "refine_degree": omx["refine_degree"],
                       "refine_degree_fp32": omx["refine_degree_fp32"], "fp32_tol": args.fp32_tol,
@@ -599,6 +605,7 @@ def profile_case(args):
         else:
             modes = {"fp64": (native.TRL_MODE_FP64, {}), "fp32": (native.TRL_MODE_FP32, {}), "mixed": (native.TRL_MODE_MIXED, {}),
                      "mixed-lanczos": (native.TRL_MODE_MIXED, {"refine": native.TRL_REFINE_LANCZOS}),
+                     "mixed-chebyshev": (native.TRL_MODE_MIXED, {"refine": native.TRL_REFINE_CHEBYSHEV}),
                      "fp64-fullreorth": (native.TRL_MODE_FP64, {"reorth": native.TRL_REORTH_CGS_IFNEEDED}),
                      "fp64-cgs2": (native.TRL_MODE_FP64, {"reorth": native.TRL_REORTH_CGS2})}
             for name in args.modes.split(","):

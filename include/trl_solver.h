@@ -13,7 +13,7 @@
  *                   and residuals in FP64. Accuracy is limited by FP32 storage.
  *   TRL_MODE_MIXED  TRL_MODE_FP32 to fp32_tol, then an FP64 refinement of the FP32 phase's
  *                   kept Ritz vectors (nev/bs + 1 blocks, widened to FP64) to `tol`:
- *                   TRL_REFINE_CHEBYSHEV (default): Rayleigh-Ritz on those vectors
+ *                   TRL_REFINE_CHEBYSHEV: Rayleigh-Ritz on those vectors
  *                     alternated with Chebyshev-filtered subspace iteration on them (the
  *                     filter damps the spectrum beyond the kept Ritz values: the interval
  *                     from the far Gershgorin bound to them when they lie on one side of
@@ -38,7 +38,12 @@ enum trl_mode { TRL_MODE_FP64 = 0, TRL_MODE_FP32 = 1, TRL_MODE_MIXED = 2 };
  * Gram-Schmidt variants (include/trl/impl/cuda/reorthogonalization.hh). */
 enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEEDED = 2, TRL_REORTH_CGS1 = 3, TRL_REORTH_PARTIAL = 4 };
 /* FP64 refinement of the mixed mode. */
-enum trl_refine { TRL_REFINE_LANCZOS = 0, TRL_REFINE_CHEBYSHEV = 1 };
+/* FP64 refinement of the mixed mode. TRL_REFINE_AUTO (default): the Chebyshev refinement
+ * after its first Rayleigh-Ritz step predicts its own time (degrees to the tolerance at the
+ * predicted rate x one measured multi-block SpMM) and hands over to the Lanczos refinement
+ * when that is predicted cheaper (estimated from the FP32 phase's time and the orders of
+ * magnitude left). */
+enum trl_refine { TRL_REFINE_LANCZOS = 0, TRL_REFINE_CHEBYSHEV = 1, TRL_REFINE_AUTO = 2 };
 
 typedef struct trl_solve_params {
   int bs;                        /* block size: 1, 2, 4, 8, 16 */
@@ -85,6 +90,9 @@ typedef struct trl_solve_info {
   unsigned refine_rounds;   /* TRL_REFINE_CHEBYSHEV: Rayleigh-Ritz rounds (0: not used) */
   unsigned refine_degree;   /* TRL_REFINE_CHEBYSHEV: total filter degree */
   unsigned refine_degree_fp32; /* TRL_REFINE_CHEBYSHEV: of which applied in FP32 */
+  int refine_used;              /* TRL_MODE_MIXED: the refinement that ran (trl_refine) */
+  double refine_predicted_s;    /* TRL_REFINE_AUTO: the Chebyshev refinement's predicted time */
+  double refine_lanczos_estimate_s; /* TRL_REFINE_AUTO: the Lanczos refinement's estimated time */
 } trl_solve_info;
 
 void trl_solve_params_default(trl_solve_params* p);

@@ -370,3 +370,26 @@ def test_zipf_fp64_matches_the_reference_on_an_indefinite_spectrum():
     assert np.max(np.abs(out["evals"] - r) / np.abs(r)) < 1e-10
     assert out["max_theta_residual"] < 1e-9
     assert abs(out["restarts"] - ref["restarts"]) <= max(3, ref["restarts"] // 5)
+
+
+@pytest.mark.parametrize("case", ["laplace2d", "zipf"])
+def test_mixed_auto_refinement_chooses_and_converges(oracle, case):
+    """TRL_REFINE_AUTO (the default) predicts the Chebyshev refinement's time after its first
+    Rayleigh-Ritz step and hands over to the Lanczos refinement when that is estimated
+    cheaper; either way the eigenpairs reach the FP64 tolerance and agree with the oracle."""
+    if case == "laplace2d":
+        A, bs, nev, ncv = P.laplace2d(128), 4, 10, 160
+    else:
+        A, bs, nev, ncv = P.zipf_symmetric(20_000, seed=7), 8, 16, 128
+    X0 = P.initial_block(A.n, bs, seed=11)
+    ref = oracle.solve_csr(A, bs, nev, ncv, X0, tol=1e-10)
+    out = native.solve_csr_host(A, X0, bs=bs, nev=nev, ncv=ncv, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4)
+    assert out["converged"]
+    assert out["refine_used"] in (native.TRL_REFINE_CHEBYSHEV, native.TRL_REFINE_LANCZOS)
+    assert out["refine_predicted_s"] > 0 and out["refine_lanczos_estimate_s"] > 0
+    if out["refine_used"] == native.TRL_REFINE_LANCZOS:
+        assert out["refine_predicted_s"] > out["refine_lanczos_estimate_s"] and out["restarts"] > 0
+    else:
+        assert out["refine_rounds"] >= 1
+    assert np.max(np.abs(out["evals"] - ref["evals"][:nev]) / np.abs(ref["evals"][:nev])) < 1e-10
+    assert out["max_theta_residual"] < 1e-10

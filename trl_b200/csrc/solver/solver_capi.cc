@@ -166,6 +166,7 @@ struct RefineOut {
   unsigned rounds = 0;
   unsigned degree = 0;   // total filter degree (FP32 and FP64 rounds)
   unsigned degree32 = 0; // of which FP32
+  double predicted_s = 0.0; // TRL_REFINE_AUTO: the filter's predicted time
   std::vector<double> evals; // Ritz values of the last Rayleigh-Ritz step, |theta| descending
 };
 
@@ -200,8 +201,11 @@ public:
   }
 
   /// X: kr blocks (device, FP64) of approximate Ritz vectors; on exit the Ritz vectors of
-  /// the last Rayleigh-Ritz step, |theta| descending.
-  RefineOut run(double* X)
+  /// the last Rayleigh-Ritz step, |theta| descending. lanczos_estimate_s > 0: before the
+  /// first filter round the refinement compares its own predicted time with this estimate of
+  /// the Lanczos refinement's and gives up (applicable = false, X the Rayleigh-Ritz vectors)
+  /// when the filter would take longer.
+  RefineOut run(double* X, double lanczos_estimate_s = 0.0)
   {
     RefineOut out;
     double lo = 0.0, hi = 0.0;
@@ -244,6 +248,15 @@ public:
       if (!(e > 0.0) || !(worst > b)) return finish(out, cur, X); // not applicable
       const double xw = (worst - c) / e, xt = (top - c) / e;
       const double rw = std::acosh(xw), rt = std::acosh(std::max(xt, xw));
+      if (round == 0 && lanczos_estimate_s > 0.0) {
+        // predicted filter time: the degrees to reach the tolerance at the predicted rate
+        // (optimistic early on, so this errs towards the filter) times one degree, measured
+        // as the Rayleigh-Ritz step's multi-block SpMM (each degree is one such SpMM plus a
+        // share of re-orthonormalisation and Rayleigh-Ritz steps, counted as 25% more)
+        const double degrees = std::log(std::max(res / p_.tol, 1.0)) / rw;
+        out.predicted_s = 1.25 * degrees * t_spmm_;
+        if (out.predicted_s > lanczos_estimate_s) return finish(out, cur, X); // not applicable: the Lanczos refinement is cheaper
+      }
       // FP32 rounds while the residual is above what FP32 vectors resolve and FP32 rounds
       // still make progress (a round that gains less than 1.05x has met the FP32 floor)
       if (use32 && prev_res > 0.0 && !(res < prev_res / 1.05)) use32 = false;
@@ -315,6 +328,7 @@ private:
   trl_cuda_handle h_;
   const trl_csr* A_;
   std::shared_ptr<const SellOp> op64_, op32_;
+  double t_spmm_ = 0.0; // seconds of one multi-block SpMM over the kept blocks
   trl_solve_params p_;
   unsigned kr_;
   std::int64_t n_;
@@ -360,7 +374,14 @@ private:
     double* AX = static_cast<double*>(AX_.get());
     double* T = static_cast<double*>(T_.get());
     double* C = static_cast<double*>(C_.get());
-    op64_->spmm(X, AX, static_cast<int>(kr_), p_.alpha, p_.beta);
+    if (t_spmm_ == 0.0) { // the first call times one multi-block SpMM (the cost of a filter degree)
+      EventTimer t(static_cast<cudaStream_t>(trl_cuda_stream(h_)));
+      t.start();
+      op64_->spmm(X, AX, static_cast<int>(kr_), p_.alpha, p_.beta);
+      t_spmm_ = t.stop();
+    }
+    else
+      op64_->spmm(X, AX, static_cast<int>(kr_), p_.alpha, p_.beta);
     // lower block triangle of H: column j = X^T (op X_j), blocks k >= j
     for (unsigned j = 0; j < kr_; ++j) {
       ctx_->check(trl_cuda_block_dot(h_, TRL_F64, X, static_cast<int>(kr_), blockp(AX, j), n_, bs, C), "refine Rayleigh-Ritz");
@@ -497,12 +518,19 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
       // direction to FP32 accuracy).
       ctx->check(trl_cuda_convert(h, TRL_F64, X64.get(), TRL_F32, X32.get(), n * bs * k32), "widen");
       bool refined = false;
-      if (p.refine == TRL_REFINE_CHEBYSHEV) {
+      if (p.refine == TRL_REFINE_CHEBYSHEV || p.refine == TRL_REFINE_AUTO) {
         ChebyshevRefinement<bs> cheb(ctx, A64, op64, p.refine_fp32 ? op32 : nullptr, p, k32);
         stage("refinement buffers allocated");
-        const RefineOut r = cheb.run(static_cast<double*>(X64.get()));
+        // TRL_REFINE_AUTO: the Lanczos refinement is estimated from the FP32 phase, which
+        // took t32 to gain log(1/fp32_tol) orders; the FP64 phase gains log(1/tol) orders at
+        // about 1.5 times the FP32 cost per step
+        const double lanczos_s = p.refine == TRL_REFINE_AUTO ? 1.5 * t32 * std::log(1.0 / p.tol) / std::log(1.0 / std::max(p.fp32_tol, 1e-7)) : 0.0;
+        const RefineOut r = cheb.run(static_cast<double*>(X64.get()), lanczos_s);
         stage("refinement done");
+        info->refine_predicted_s = r.predicted_s;
+        info->refine_lanczos_estimate_s = lanczos_s;
         if (r.applicable) {
+          info->refine_used = TRL_REFINE_CHEBYSHEV;
           refined = true;
           out.converged = r.converged;
           out.restarts = 0;
@@ -514,6 +542,7 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
         }
       }
       if (!refined) {
+      info->refine_used = TRL_REFINE_LANCZOS;
       std::vector<double> G(static_cast<std::size_t>(kr) * bs * bs);
       std::mt19937 rng(p.seed);
       std::normal_distribution<double> dist;
@@ -637,7 +666,7 @@ void validate(const trl_solve_params* p)
   if (p->cholqr_passes < 1 || p->cholqr_passes > 4) throw std::invalid_argument("cholqr_passes must be in [1, 4]");
   if (p->reorth < TRL_REORTH_MGS || p->reorth > TRL_REORTH_PARTIAL) throw std::invalid_argument("bad reorth strategy");
   if (!(p->partial_threshold >= 0.0)) throw std::invalid_argument("partial_threshold must be >= 0");
-  if (p->refine != TRL_REFINE_LANCZOS && p->refine != TRL_REFINE_CHEBYSHEV) throw std::invalid_argument("bad refinement");
+  if (p->refine != TRL_REFINE_LANCZOS && p->refine != TRL_REFINE_CHEBYSHEV && p->refine != TRL_REFINE_AUTO) throw std::invalid_argument("bad refinement");
 }
 
 } // namespace
@@ -663,7 +692,7 @@ void trl_solve_params_default(trl_solve_params* p)
   p->want_vectors = 1;
   p->batching = 1;
   p->seed = 42;
-  p->refine = TRL_REFINE_CHEBYSHEV;
+  p->refine = TRL_REFINE_AUTO;
   p->refine_fp32 = 1;
   p->partial_pairs = 1; // 96^3 workload: 242 of 3058 steps projected, 1.25 s; 822 steps and 1.56 s without
 }

@@ -25,7 +25,7 @@ TRL_MULT, TRL_MULT_TRANSPOSE, TRL_MULT_ADD, TRL_SUBTRACT, TRL_SUBTRACT_TRANSPOSE
 TRL_MODE_FP64, TRL_MODE_FP32, TRL_MODE_MIXED = 0, 1, 2
 TRL_REORTH_MGS, TRL_REORTH_CGS2, TRL_REORTH_CGS_IFNEEDED, TRL_REORTH_CGS1, TRL_REORTH_PARTIAL = 0, 1, 2, 3, 4
 TRL_CGS_ONE, TRL_CGS_TWO, TRL_CGS_IFNEEDED = 0, 1, 2
-TRL_REFINE_LANCZOS, TRL_REFINE_CHEBYSHEV = 0, 1
+TRL_REFINE_LANCZOS, TRL_REFINE_CHEBYSHEV, TRL_REFINE_AUTO = 0, 1, 2
 
 P = C.c_void_p
 I64 = C.c_int64
@@ -106,7 +106,8 @@ class trl_solve_info(C.Structure):
                 ("seconds_vectors", C.c_double), ("max_rel_residual", C.c_double), ("max_theta_residual", C.c_double),
                 ("op_norm1", C.c_double), ("kernel_launches", C.c_ulonglong), ("h2d_bytes", C.c_double), ("d2h_bytes", C.c_double),
                 ("refine_rounds", C.c_uint), ("refine_degree", C.c_uint),
-                ("refine_degree_fp32", C.c_uint)]
+                ("refine_degree_fp32", C.c_uint), ("refine_used", C.c_int), ("refine_predicted_s", C.c_double),
+                ("refine_lanczos_estimate_s", C.c_double)]
 
 
 SOLVER_SYMBOLS = {
