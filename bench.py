@@ -582,7 +582,8 @@ def profile_case(args):
     project      one Gram-Schmidt pass as the solver issues it, against --nblk blocks;
     rotate       the thick-restart rotation V (48 blocks) x Y -> 5 blocks;
     small-eigen  the projected eigenproblem of a thick-restart matrix (N = --nblk x 8, the
-                 kept 40 eigenvectors), --reps calls.
+                 kept 40 eigenvectors), --reps calls;
+    dmma-peak    the FP64 tensor-core (DMMA) throughput of the GPU (trl_cuda_measure_dmma_rate).
     Every case on the default workload reads and writes more than the 126 MB L2 and holds at
     most a few GB."""
     import torch
@@ -686,6 +687,10 @@ def profile_case(args):
         W = torch.empty(5, A.n, bs, dtype=dt, device="cuda")
         for _ in range(args.reps):
             h.block_rotate(V, Y, 5, W)
+    elif args.case == "dmma-peak":
+        tf = native.C.c_double(0.0)
+        h.check(h.lib.trl_cuda_measure_dmma_rate(h.h, native.C.byref(tf)))
+        print(json.dumps({"case": "dmma-peak", "tflops": tf.value, "how": "independent DMMA m8n8k4 chains on every SM, CUDA events"}), flush=True)
     elif args.case == "small-eigen":
         # a thick-restart projected matrix (lanczos.hh:119-150): kept Ritz values on the
         # diagonal, their coupling to the next block, block-tridiagonal below
@@ -723,7 +728,7 @@ def main():
     ap.add_argument("--workloads", default="aniso96,elast64,zipf4m", help="headline workload plus the secondary ones solved once per mode")
     ap.add_argument("--secondary-modes", default="fp64,mixed")
     ap.add_argument("--cpu-cycles", type=int, default=0, help=argparse.SUPPRESS)  # child process of the CPU legs
-    ap.add_argument("--case", choices=["solve", "mixed", "solves", "spmm", "spmm-csr", "spmm-rates", "dot", "update", "project", "rotate", "small-eigen"],
+    ap.add_argument("--case", choices=["solve", "mixed", "solves", "spmm", "spmm-csr", "spmm-rates", "dot", "update", "project", "rotate", "small-eigen", "dmma-peak"],
                     default=None, help="profiling driver: run one piece of a workload and exit (see profile_case)")
     ap.add_argument("--workload", default="aniso96", choices=["aniso96", "elast64", "zipf4m"])
     ap.add_argument("--modes", default="fp64,mixed")

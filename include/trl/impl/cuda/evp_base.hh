@@ -60,6 +60,28 @@ public:
 
   virtual void orthonormalize(BlockView V, BlockMatrixBlockView R)
   {
+    if (!euclidean_dot()) {
+      // Cholesky-QR in the eigenproblem's own inner product, as the reference does it
+      // (evp_base.hh:39-71: G = dot(V, V), G = U^T U, V <- V U^{-1}, R = U), repeated
+      // cholqr_passes times with R accumulated (R <- U_2 U_1)
+      if (!mgram_.get()) mgram_ = DeviceBuffer(ctx_, 3 * kCoefBytes);
+      double* G = static_cast<double*>(mgram_.get());
+      double* Rp = G + blocksize * blocksize;
+      double* Rt = Rp + blocksize * blocksize;
+      for (int pass = 0; pass < cholqr_passes_; ++pass) {
+        this->dot(V, V, BlockMatrixBlockView(ctx_.get(), G));
+        const std::size_t blk = sizeof(Storage) * N * blocksize;
+        ctx_->prepare({{V.data_, blk, false}, {V.data_, blk, true}, {R.data_, kCoefBytes, true}, {G, 3 * kCoefBytes, true}});
+        double* out = pass == 0 ? R.data_ : Rp;
+        ctx_->check(trl_cuda_cholqr_gram(ctx_->handle(), dtype, V.data_, static_cast<std::int64_t>(N), blocksize, 1, out, G), "orthonormalize");
+        if (pass > 0) {
+          ctx_->check(trl_cuda_mb_mult(ctx_->handle(), Rp, R.data_, Rt, blocksize), "orthonormalize");
+          ctx_->check(trl_cuda_mb_copy(ctx_->handle(), R.data_, Rt, blocksize, 0), "orthonormalize");
+        }
+      }
+      gram_block_ = nullptr;
+      return;
+    }
     // The Gram matrix V^T V is reused when the reorthogonalisation that just ran on this
     // very block formed it (and no other operation ran since).
     const bool reuse = gram_block_ == V.data_ && gram_seq_ == ctx_->seq();
@@ -281,6 +303,7 @@ protected:
   std::unique_ptr<BlockMatrix> eigenvectors;
   DeviceBuffer evals_dev_;
   DeviceBuffer gram_;                  // Gram matrix of the last reorthogonalised block
+  DeviceBuffer mgram_;                 // non-Euclidean orthonormalize: Gram, pass factor, product
   const Storage* gram_block_ = nullptr; // ... which block it belongs to
   std::uint64_t gram_seq_ = 0;         // ... and the operation sequence number it was made at
 

@@ -86,6 +86,11 @@ uint64_t trl_cuda_launch_count(trl_cuda_handle handle);
 int trl_cuda_inject_alloc_failures(trl_cuda_handle handle, int count);
 int trl_cuda_test_bounded_wait(trl_cuda_handle handle, unsigned polls);
 
+/* FP64 tensor-core (DMMA m8n8k4) throughput of this GPU, measured with a loop of independent
+ * DMMA chains on every SM (CUDA events; synchronises): the denominator of the contraction
+ * kernels' tensor-pipe fraction. Diagnostics; no counterpart in the reference. */
+int trl_cuda_measure_dmma_rate(trl_cuda_handle handle, double* host_tflops);
+
 /* ---- per-kernel-class device timing ---------------------------------------------------
  * When enabled, every outermost C-ABI call is bracketed by CUDA events on the handle's
  * stream and credited with its algorithmic bytes (data each operand must move once) and

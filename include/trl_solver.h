@@ -113,6 +113,15 @@ int trl_solve_csr_host(const trl_solve_params* p, int device, int64_t n, int64_t
 int trl_solve_csr_device(trl_cuda_handle h, const trl_solve_params* p, const trl_csr* A64, const trl_csr* A32, const double* X0, double* evals_host, double* evecs_dev,
                          double* resid_host, trl_solve_info* info);
 
+/* Eigenpairs of an operator that is self-adjoint in the inner product <x, y> = x^T M y (M SPD,
+ * device CSR, FP64), e.g. op = M^{-1} K for K x = lambda M x: BlockLanczos with dot(V, W) =
+ * V^T (M W) and Cholesky-QR in that inner product, as the reference's generalised example
+ * (examples/openmp/csrevp.hh:52-109, whose operator is (A - sigma B)^{-1} B through a sparse
+ * LU; here the operator is given as a CSR matrix). FP64 only (p->mode = TRL_MODE_FP64);
+ * eigenvectors are M-orthonormal; resid = ||op x - theta x||_2 / (||op||_1 ||x||_2). */
+int trl_solve_csr_minner_device(trl_cuda_handle h, const trl_solve_params* p, const trl_csr* op, const trl_csr* M, const double* X0, double* evals_host, double* evecs_dev,
+                                double* resid_host, trl_solve_info* info);
+
 const char* trl_solver_last_error(void);
 
 /* Matrix Market coordinate file -> CSR in full storage, in host memory allocated with

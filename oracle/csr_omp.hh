@@ -71,4 +71,35 @@ private:
   double alpha_, beta_;
 };
 
+/// The generalised eigenproblem of the reference's example (examples/openmp/csrevp.hh:52-109)
+/// with its operator given explicitly as a CSR matrix (there: (A - sigma B)^{-1} B through
+/// Eigen's SparseLU, which is not available here) and its inner product dot = V^T (B W)
+/// (:89-97), B a CSR matrix. The restated EVPBase orthonormalizes through dot(), as the
+/// reference's does (evp_base.hh:43-50).
+template <class T, unsigned int bs>
+class CSRMInnerEVP : public CSREVP<T, bs> {
+public:
+  using Base = CSREVP<T, bs>;
+  using BlockView = typename Base::BlockView;
+
+  CSRMInnerEVP(std::size_t n, const std::int32_t* rowptr, const std::int32_t* colind, const double* values, const std::int32_t* mrow, const std::int32_t* mcol,
+               const double* mval)
+      : Base(n, rowptr, colind, values)
+      , M_(n, mrow, mcol, mval)
+      , tmp_(n * bs)
+  {
+  }
+
+  void dot(BlockView V, BlockView W, typename Base::BlockMatrixBlockView R) override
+  {
+    BlockView Tview(tmp_.data(), this->size());
+    M_.apply(W, Tview);
+    V.dot(Tview, R);
+  }
+
+private:
+  CSREVP<T, bs> M_;
+  std::vector<T> tmp_;
+};
+
 } // namespace trl_oracle

@@ -47,6 +47,7 @@ def lib():
         L.oracle_last_error.restype = C.c_char_p
         L.oracle_solve_csr.argtypes = [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_double, C.c_uint, C.c_uint, C.c_uint, C.c_double, P, P, P, P, P, P]
         L.oracle_block_view_op.argtypes = [C.c_int, C.c_int, C.c_int64, P, P, P]
+        L.oracle_solve_csr_minner.argtypes = [C.c_int, C.c_int64, P, P, P, P, P, P, C.c_uint, C.c_uint, C.c_uint, C.c_double, P, P, P, P]
         L.oracle_orthonormalize.argtypes = [C.c_int, C.c_int64, P, P]
         L.oracle_solve_small_dense.argtypes = [C.c_int, C.c_uint, P, P, C.c_uint, C.c_double, P, P, P]
         L.oracle_spmm.argtypes = [C.c_int, C.c_int64, P, P, P, C.c_double, C.c_double, P, P]
@@ -88,6 +89,21 @@ def solve_csr(A, bs: int, nev: int, ncv: int, X0: np.ndarray, tol: float = 1e-8,
                                   _p(evals), _p(ritz_vecs), _p(stats), _p(secs), _p(cycles)))
     return {"converged": bool(stats[0]), "iterations": int(stats[1]), "n_op_apply": int(stats[2]),
             "seconds": float(secs[0]), "evals": evals, "ritz": ritz_vecs, "cycle_seconds": cycles[: int(stats[1])].copy()}
+
+
+def solve_csr_minner(A, M, bs: int, nev: int, ncv: int, X0: np.ndarray, tol: float = 1e-10, max_restarts: int = 1000) -> dict:
+    """The reference BlockLanczos (ModifiedGS) on the operator A with dot = V^T (M W) and
+    CholQR in that inner product (the reference's generalised example's inner product,
+    examples/openmp/csrevp.hh:89-97). Returns eigenvalues and M-orthonormal Ritz vectors."""
+    n = A.n
+    X0 = np.ascontiguousarray(X0, dtype=np.float64).reshape(n, bs)
+    evals = np.zeros(ncv)
+    ritz = np.zeros((n, nev))
+    stats = np.zeros(3, dtype=np.int32)
+    arrs = [np.ascontiguousarray(a, dtype=t) for a, t in ((A.rowptr, np.int32), (A.colind, np.int32), (A.values, np.float64),
+                                                         (M.rowptr, np.int32), (M.colind, np.int32), (M.values, np.float64))]
+    _check(lib().oracle_solve_csr_minner(bs, n, *[_p(a) for a in arrs], nev, ncv, max_restarts, tol, _p(X0), _p(evals), _p(ritz), _p(stats)))
+    return {"converged": bool(stats[0]), "iterations": int(stats[1]), "n_op_apply": int(stats[2]), "evals": evals, "ritz": ritz}
 
 
 def block_view_op(bs: int, op: int, X: np.ndarray, Y: np.ndarray, W: np.ndarray) -> None:

@@ -96,6 +96,41 @@ int solve_csr(std::int64_t n, const std::int32_t* rowptr, const std::int32_t* co
   return 0;
 }
 
+// The reference driver on the M-inner-product eigenproblem (trl_oracle::CSRMInnerEVP); Ritz
+// vectors (M-orthonormal) into ritz_out (n x nev) when given.
+template <unsigned bs>
+int solve_minner(std::int64_t n, const std::int32_t* rowptr, const std::int32_t* colind, const double* values, const std::int32_t* mrow, const std::int32_t* mcol,
+                 const double* mval, unsigned nev, unsigned ncv, unsigned max_restarts, double tol, const double* X0, double* evals_out, double* ritz_out, std::int32_t* stats)
+{
+  using EVP = trl_oracle::CSRMInnerEVP<double, bs>;
+  auto evp = std::make_shared<EVP>(static_cast<std::size_t>(n), rowptr, colind, values, mrow, mcol, mval);
+  trl::EigensolverParams params{.nev = nev, .ncv = ncv, .max_restarts = max_restarts, .tolerance = tol};
+  trl::BlockLanczos lanczos(evp, params);
+  std::memcpy(lanczos.initial_block().data_, X0, sizeof(double) * static_cast<std::size_t>(n) * bs);
+  const auto res = lanczos.solve();
+  stats[0] = res.converged ? 1 : 0;
+  stats[1] = static_cast<std::int32_t>(res.iterations);
+  stats[2] = static_cast<std::int32_t>(res.n_op_apply);
+  const auto& ev = evp->get_current_eigenvalues();
+  for (std::size_t i = 0; i < ev.size() && i < ncv; ++i) evals_out[i] = ev[i];
+  if (ritz_out) {
+    const auto& Y = evp->get_current_eigenvectors();
+    auto& V = lanczos.get_basis();
+    const std::size_t m = ncv / bs, N = static_cast<std::size_t>(n);
+    for (std::size_t r = 0; r < N; ++r)
+      for (unsigned c = 0; c < nev; ++c) {
+        double s = 0.0;
+        for (std::size_t i = 0; i < m; ++i) {
+          const double* vi = V.block_view(i).data_ + r * bs;
+          const double* yb = Y.block_view(i, c / bs).data_;
+          for (unsigned l = 0; l < bs; ++l) s += vi[l] * yb[l * bs + (c % bs)];
+        }
+        ritz_out[r * nev + c] = s;
+      }
+  }
+  return 0;
+}
+
 template <unsigned bs>
 int bv_op(int op, std::int64_t n, double* X, double* Y, double* W)
 {
@@ -164,6 +199,11 @@ struct SolveF {
   static int run(A... a) { return solve_csr<bs>(a...); }
 };
 template <unsigned bs>
+struct MInnerF {
+  template <class... A>
+  static int run(A... a) { return solve_minner<bs>(a...); }
+};
+template <unsigned bs>
 struct BvF {
   template <class... A>
   static int run(A... a) { return bv_op<bs>(a...); }
@@ -206,6 +246,13 @@ int oracle_solve_csr(int bs, std::int64_t n, const std::int32_t* rowptr, const s
   return guarded([&] {
     return dispatch_bs<SolveF>(bs, n, rowptr, colind, values, alpha, beta, nev, ncv, max_restarts, tol, X0, evals_out, ritz_out, stats, seconds, cycle_seconds);
   });
+}
+
+int oracle_solve_csr_minner(int bs, std::int64_t n, const std::int32_t* rowptr, const std::int32_t* colind, const double* values, const std::int32_t* mrow,
+                            const std::int32_t* mcol, const double* mval, unsigned nev, unsigned ncv, unsigned max_restarts, double tol, const double* X0,
+                            double* evals_out, double* ritz_out, std::int32_t* stats)
+{
+  return guarded([&] { return dispatch_bs<MInnerF>(bs, n, rowptr, colind, values, mrow, mcol, mval, nev, ncv, max_restarts, tol, X0, evals_out, ritz_out, stats); });
 }
 
 int oracle_block_view_op(int bs, int op, std::int64_t n, double* X, double* Y, double* W)

@@ -127,3 +127,21 @@ def test_golden_vectors(oracle):
     r = oracle.solve_csr(A, 4, 6, 24, g["solve_X0"], tol=1e-10)
     assert np.allclose(r["evals"][:6], g["solve_evals"], rtol=1e-12)
     assert r["iterations"] == int(g["solve_iterations"])
+
+
+def test_oracle_minner_solves_the_generalised_problem(oracle):
+    """The reference driver with dot = V^T (M W) (examples/openmp/csrevp.hh:89-97) on
+    op = M^{-1} K with a non-diagonal SPD M gives the generalised eigenpairs of (K, M) with
+    M-orthonormal Ritz vectors."""
+    import scipy.linalg as sl
+
+    K, M = P.diffusion2d_consistent_mass(12, seed=3)
+    Kd, Md = K.to_dense(), M.to_dense()
+    Op = P.dense_csr(np.linalg.solve(Md, Kd))
+    X0 = P.initial_block(K.n, 4, seed=5)
+    r = oracle.solve_csr_minner(Op, M, 4, 8, 48, X0, tol=1e-10)
+    assert r["converged"]
+    lam = sl.eigh(Kd, Md, eigvals_only=True)[::-1][:8]
+    assert np.max(np.abs(r["evals"][:8] - lam) / lam) < 1e-10
+    X = r["ritz"]
+    assert np.abs(X.T @ Md @ X - np.eye(8)).max() < 1e-10

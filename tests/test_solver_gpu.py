@@ -393,3 +393,31 @@ def test_mixed_auto_refinement_chooses_and_converges(oracle, case):
         assert out["refine_rounds"] >= 1
     assert np.max(np.abs(out["evals"] - ref["evals"][:nev]) / np.abs(ref["evals"][:nev])) < 1e-10
     assert out["max_theta_residual"] < 1e-10
+
+
+@pytest.mark.parametrize("bs,reorth", [(4, native.TRL_REORTH_CGS_IFNEEDED), (4, native.TRL_REORTH_MGS), (2, native.TRL_REORTH_PARTIAL), (8, native.TRL_REORTH_CGS2)])
+def test_m_inner_product_matches_the_oracle(oracle, bs, reorth):
+    """K x = lambda M x with a non-diagonal SPD M through op = M^{-1} K (self-adjoint in the M
+    inner product): dot = V^T (M W) and CholQR in that inner product on the device, against
+    the reference driver with the same inner product (the oracle) and a dense generalised
+    eigensolver; Ritz vectors M-orthonormal."""
+    import scipy.linalg as sl
+
+    K, M = P.diffusion2d_consistent_mass(12, seed=3)
+    Kd, Md = K.to_dense(), M.to_dense()
+    Op = P.dense_csr(np.linalg.solve(Md, Kd))
+    nev, ncv = 8, 12 * bs
+    X0 = P.initial_block(K.n, bs, seed=5)
+    ref = oracle.solve_csr_minner(Op, M, bs, nev, ncv, X0, tol=1e-10)
+    h = native.Handle(0)
+    ev = torch.zeros((K.n, nev), dtype=torch.float64, device="cuda")
+    out = native.solve_csr_minner_device(h, native.DeviceCSRTensors.from_host(Op), native.DeviceCSRTensors.from_host(M), torch.from_numpy(X0).cuda(), evecs=ev,
+                                         bs=bs, nev=nev, ncv=ncv, tol=1e-10, reorth=reorth)
+    assert out["converged"] and ref["converged"]
+    lam = sl.eigh(Kd, Md, eigvals_only=True)[::-1][:nev]
+    assert np.max(np.abs(out["evals"] - ref["evals"][:nev]) / lam) < 1e-10
+    assert np.max(np.abs(out["evals"] - lam) / lam) < 1e-10
+    X = ev.cpu().numpy()
+    assert np.abs(X.T @ Md @ X - np.eye(nev)).max() < 1e-9
+    assert out["max_theta_residual"] < 1e-9
+    h.close()

@@ -1542,3 +1542,53 @@ extern "C" int trl_cuda_block_dot_noalloc(void* stream, int dtype, const void* V
   TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, st = noalloc_dot_dispatch<T, BS>(s, sms, partial, static_cast<const T*>(V), nblk, static_cast<const T*>(W), n, C)));
   return st;
 }
+
+namespace {
+
+// FP64 tensor-core (DMMA m8n8k4) issue rate: every warp runs kDmmaChains independent
+// accumulator chains for `iters` rounds; the result is written so that nothing is elided.
+constexpr int kDmmaChains = 8;
+
+__global__ void __launch_bounds__(256) k_dmma_rate(int iters, double* __restrict__ out)
+{
+  double d0[kDmmaChains], d1[kDmmaChains];
+  const double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * blockIdx.x;
+#pragma unroll
+  for (int c = 0; c < kDmmaChains; ++c) d0[c] = d1[c] = 0.0;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int c = 0; c < kDmmaChains; ++c) dmma_m8n8k4(d0[c], d1[c], a, b);
+  double s = 0.0;
+#pragma unroll
+  for (int c = 0; c < kDmmaChains; ++c) s += d0[c] + d1[c];
+  if (s == 12345.678) out[0] = s; // never true; keeps the chains alive
+}
+
+} // namespace
+
+extern "C" int trl_cuda_measure_dmma_rate(trl_cuda_handle h, double* host_tflops)
+{
+  TRL_CHECK_HANDLE(h);
+  if (!host_tflops) return set_error(h, TRL_EINVAL, "null output");
+  double* out = static_cast<double*>(small_scratch(h));
+  if (!out) return TRL_ENOMEM;
+  const int iters = 4096;
+  const unsigned grid = static_cast<unsigned>(h->num_sms) * 8;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_dmma_rate<<<grid, 256, 0, h->stream>>>(iters, out); // warm-up
+  cudaEventRecord(a, h->stream);
+  k_dmma_rate<<<grid, 256, 0, h->stream>>>(iters, out);
+  cudaEventRecord(b, h->stream);
+  const cudaError_t e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) return set_error(h, TRL_ECUDA, "dmma rate: %s", cudaGetErrorString(e));
+  if (int st = after_launch(h, "dmma rate")) return st;
+  const double flops = 2.0 * 8 * 8 * 4 * kDmmaChains * static_cast<double>(iters) * grid * (256 / 32);
+  *host_tflops = flops / (ms * 1e-3) / 1e12;
+  return TRL_OK;
+}

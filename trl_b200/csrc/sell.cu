@@ -270,12 +270,17 @@ constexpr int kSpmmWarps = kSpmmThreads / 32;
 // SpMM; the multi-block SpMM takes two blocks per pass and re-reads a slice's indices and
 // values, from L2, for each pair), UG slots per group, and the CTAs per SM the registers
 // must allow.
-template <typename T, int BS, int NBG>
+template <typename T, int BS, int NBG, bool LONG>
 struct SellTune {
   static constexpr int lane_bytes = SellShape<T, BS>::VEC * static_cast<int>(sizeof(T));
   static constexpr int ug = 64 / lane_bytes;
-  static constexpr int UG = NBG == 1 ? (ug > 4 ? 4 : ug) : 2;
-  static constexpr int MINB = NBG == 1 ? 4 : 2;
+  // operators with long rows (LONG: 16 or more slots per slice on average) keep 8 slots of
+  // gathers in flight per lane at two CTAs per SM; short rows prefer more warps with fewer
+  // slots each (measured on B200: 96^3 stencil, 7 slots per slice, 0.56 of the copy peak
+  // with 2 slots x 4 CTAs against 0.53 with 8 x 2; elasticity, 81 slots, 0.50 with 8 x 2
+  // against 0.39 with 2 x 4)
+  static constexpr int UG = NBG == 1 ? (LONG ? 8 : (ug > 4 ? 4 : ug)) : 2;
+  static constexpr int MINB = NBG == 1 ? (LONG ? 2 : 4) : 2;
 };
 
 // Asks L2 to fetch [p, p + bytes) (a bulk prefetch: no registers, no shared memory). p and
@@ -293,13 +298,13 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes)
 // loads the column indices of group g + 1, which may belong to the next slice. The bounds
 // and rows of the next slice are loaded one slice ahead, and lane 0 asks L2 for the slice
 // after it (bulk prefetch), so that the index loads hit L2.
-template <typename T, int BS, int NBG>
-__global__ void __launch_bounds__(kSpmmThreads, SellTune<T, BS, NBG>::MINB)
+template <typename T, int BS, int NBG, bool LONG>
+__global__ void __launch_bounds__(kSpmmThreads, SellTune<T, BS, NBG, LONG>::MINB)
     k_spmm_sell(int nslices, int nwin, int spw, int interleave, const int32_t* __restrict__ perm, const int64_t* __restrict__ sptr, const int32_t* __restrict__ scol,
                 const T* __restrict__ sval, const T* __restrict__ X, T* Y, T alpha, T beta, T gamma, const T* W, int nb, int64_t bstride)
 {
   using S = SellShape<T, BS>;
-  constexpr int VEC = S::VEC, LPR = S::LPR, C = S::RPW, UG = SellTune<T, BS, NBG>::UG;
+  constexpr int VEC = S::VEC, LPR = S::LPR, C = S::RPW, UG = SellTune<T, BS, NBG, LONG>::UG;
   const int lane = threadIdx.x & 31;
   const int grp = lane / LPR, sub = lane % LPR;
   const int wstride = static_cast<int>(gridDim.x) * kSpmmWarps;
@@ -441,6 +446,7 @@ struct trl_cuda_sell_op {
   int64_t nslices = 0, nwin = 0;
   int spw = 0;           // slices per window
   int interleave = 0;    // take slices window-major (skewed row lengths)
+  int long_rows = 0;     // 16 or more slots per slice on average
   int64_t stored = 0;    // entries including padding
   int longest = 0;       // longest row (entries)
   int32_t* perm = nullptr;
@@ -522,6 +528,7 @@ int trl_cuda_op_create(trl_cuda_handle h, const trl_csr* A, int bs, trl_cuda_op*
   // skewed row lengths (a slice far longer than the mean): spread each window's first slices
   const double mean = static_cast<double>(op->stored) / (static_cast<double>(op->nslices) * C);
   op->interleave = op->longest > 4.0 * mean + 8.0 ? 1 : 0;
+  op->long_rows = mean >= 16.0 ? 1 : 0;
   const int64_t alloc = op->stored > 0 ? op->stored : 1;
   if ((st = trl_cuda_malloc(h, &p, sizeof(int32_t) * alloc))) return fail(st);
   op->scol = static_cast<int32_t*>(p);
@@ -588,8 +595,9 @@ int trl_cuda_op_spmm(trl_cuda_handle h, trl_cuda_op op, const void* X, void* Y, 
                                                    static_cast<const T*>(X), static_cast<T*>(Y), static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma),
                                                    static_cast<const T*>(W), nb, op->n * BS);
     };
-    if (nb > 1) launch(k_spmm_sell<T, BS, 2>, SellTune<T, BS, 2>::MINB);
-    else launch(k_spmm_sell<T, BS, 1>, SellTune<T, BS, 1>::MINB);
+    if (nb > 1) launch(k_spmm_sell<T, BS, 2, false>, SellTune<T, BS, 2, false>::MINB);
+    else if (op->long_rows) launch(k_spmm_sell<T, BS, 1, true>, SellTune<T, BS, 1, true>::MINB);
+    else launch(k_spmm_sell<T, BS, 1, false>, SellTune<T, BS, 1, false>::MINB);
     st = after_launch(h, "spmm (sliced ELL)");
   }));
   return st;

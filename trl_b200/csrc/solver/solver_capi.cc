@@ -607,6 +607,103 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
   return TRL_OK;
 }
 
+// ---- matrix-weighted inner product (K x = lambda M x through an M-self-adjoint operator) --
+
+template <unsigned bs, class Reorth>
+int solve_minner_phase(const std::shared_ptr<Context>& ctx, const trl_solve_params& p, const trl_csr* op, const trl_csr* M, const double* X0, double* evals_host,
+                       double* evecs_dev, double* resid_host, trl_solve_info* info)
+{
+  using EVP = trl::cuda::MInnerCSREVP<double, bs>;
+  const auto h = ctx->handle();
+  const std::int64_t n = op->n;
+  const unsigned kx = (p.nev + bs - 1) / bs;
+  cudaStream_t stream = static_cast<cudaStream_t>(trl_cuda_stream(h));
+  EventTimer total(stream);
+  total.start();
+  const auto launches0 = trl_cuda_launch_count(h);
+  auto opd = DeviceCSR<double>::wrap(op->n, op->nnz, op->rowptr, op->colind, static_cast<const double*>(op->values));
+  auto Md = DeviceCSR<double>::wrap(M->n, M->nnz, M->rowptr, M->colind, static_cast<const double*>(M->values));
+  auto evp = std::make_shared<EVP>(ctx, std::move(opd), std::move(Md), p.alpha, p.beta);
+  evp->set_cholqr_passes(p.cholqr_passes);
+  evp->set_full_eigenvectors(p.small_eigen_full != 0);
+  evp->set_min_eigenvectors(static_cast<std::size_t>(kx) * bs);
+  trl::EigensolverParams ep{.nev = p.nev, .ncv = p.ncv, .max_restarts = p.max_restarts, .tolerance = p.tol};
+  trl::BlockLanczos<EVP, Reorth> lanczos(evp, ep);
+  auto V0 = lanczos.initial_block();
+  ctx->flush();
+  ctx->check(trl_cuda_memcpy(h, V0.data_, X0, sizeof(double) * static_cast<std::size_t>(n) * bs, TRL_D2D), "initial block");
+  const auto res = lanczos.solve();
+  ctx->flush();
+  info->converged = res.converged ? 1 : 0;
+  info->restarts = res.iterations;
+  info->n_op_apply = res.n_op_apply;
+  const auto ev = evp->get_current_eigenvalues();
+  for (unsigned c = 0; c < p.nev; ++c) evals_host[c] = c < ev.size() ? ev[c] : 0.0;
+  if (p.want_vectors) {
+    DeviceBuffer X(ctx, sizeof(double) * static_cast<std::size_t>(n) * bs * kx);
+    auto& V = lanczos.get_basis();
+    const auto& Y = evp->get_current_eigenvectors();
+    ctx->check(trl_cuda_block_rotate(h, TRL_F64, V.data(), static_cast<int>(p.ncv / bs), Y.data(), static_cast<int>(Y.block_cols()), static_cast<int>(kx), X.get(), n, bs),
+               "ritz vectors");
+    // residuals ||op x - theta x|| / ||op||_1 (Euclidean norms; x is M-normalised)
+    SellOp opsell(ctx, op, static_cast<int>(bs));
+    double norm1 = 0.0;
+    ctx->check(trl_cuda_csr_norm1(h, op, p.alpha, p.beta, &norm1), "norm");
+    info->op_norm1 = norm1;
+    DeviceBuffer R(ctx, sizeof(double) * static_cast<std::size_t>(n) * bs), D(ctx, sizeof(double) * bs * bs), G(ctx, sizeof(double) * bs * bs * 2);
+    std::vector<double> gh(2 * bs * bs);
+    for (unsigned j = 0; j < kx; ++j) {
+      const double* Xj = static_cast<const double*>(X.get()) + static_cast<std::size_t>(j) * n * bs;
+      opsell.spmm(Xj, R.get(), 1, p.alpha, p.beta);
+      double diag[16] = {0};
+      for (unsigned c = 0; c < bs; ++c) diag[c] = (j * bs + c < p.nev) ? evals_host[j * bs + c] : 0.0;
+      ctx->check(trl_cuda_mb_zero(h, static_cast<double*>(D.get()), bs), "residual");
+      ctx->check(trl_cuda_mb_set_diagonal(h, static_cast<double*>(D.get()), diag, bs), "residual");
+      ctx->check(trl_cuda_bv_mult(h, TRL_F64, TRL_SUBTRACT, Xj, static_cast<const double*>(D.get()), R.get(), n, bs), "residual");
+      ctx->check(trl_cuda_block_dot(h, TRL_F64, R.get(), 1, R.get(), n, bs, static_cast<double*>(G.get())), "residual");
+      ctx->check(trl_cuda_block_dot(h, TRL_F64, Xj, 1, Xj, n, bs, static_cast<double*>(G.get()) + bs * bs), "residual");
+      ctx->check(trl_cuda_memcpy(h, gh.data(), G.get(), sizeof(double) * 2 * bs * bs, TRL_D2H), "residual");
+      for (unsigned c = 0; c < bs && j * bs + c < p.nev; ++c) {
+        const double r_rel = std::sqrt(std::max(0.0, gh[c * bs + c])) / std::max(std::sqrt(std::max(0.0, gh[bs * bs + c * bs + c])), 1e-300);
+        if (resid_host) resid_host[j * bs + c] = r_rel / std::max(norm1, 1e-300);
+        info->max_rel_residual = std::max(info->max_rel_residual, r_rel / std::max(norm1, 1e-300));
+        info->max_theta_residual = std::max(info->max_theta_residual, r_rel / std::max(std::abs(evals_host[j * bs + c]), 1e-300));
+      }
+    }
+    if (evecs_dev) ctx->check(trl_cuda_unblock(h, static_cast<const double*>(X.get()), n, bs, static_cast<int>(p.nev), evecs_dev), "ritz vectors");
+  }
+  ctx->sync();
+  info->seconds = total.stop();
+  info->kernel_launches = trl_cuda_launch_count(h) - launches0;
+  return TRL_OK;
+}
+
+template <unsigned bs>
+int solve_minner_r(const std::shared_ptr<Context>& ctx, const trl_solve_params& p, const trl_csr* op, const trl_csr* M, const double* X0, double* ev, double* evecs, double* resid,
+                   trl_solve_info* info)
+{
+  switch (p.reorth) {
+  case TRL_REORTH_MGS: return solve_minner_phase<bs, trl::ModifiedGS>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case TRL_REORTH_CGS1: return solve_minner_phase<bs, trl::cuda::BlockCGS1>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case TRL_REORTH_CGS2: return solve_minner_phase<bs, trl::cuda::BlockCGS2>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case TRL_REORTH_PARTIAL: return solve_minner_phase<bs, trl::cuda::BlockCGSPartial>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  default: return solve_minner_phase<bs, trl::cuda::BlockCGSIfNeeded>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  }
+}
+
+int dispatch_minner(const std::shared_ptr<Context>& ctx, const trl_solve_params& p, const trl_csr* op, const trl_csr* M, const double* X0, double* ev, double* evecs,
+                    double* resid, trl_solve_info* info)
+{
+  switch (p.bs) {
+  case 1: return solve_minner_r<1>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case 2: return solve_minner_r<2>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case 4: return solve_minner_r<4>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case 8: return solve_minner_r<8>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  case 16: return solve_minner_r<16>(ctx, p, op, M, X0, ev, evecs, resid, info);
+  default: throw std::invalid_argument("unsupported block size " + std::to_string(p.bs));
+  }
+}
+
 int dispatch(const std::shared_ptr<Context>& ctx, const trl_solve_params& p, const trl_csr* A64, const trl_csr* A32, const double* X0, double* evals_host, double* evecs_dev,
              double* resid_host, trl_solve_info* info)
 {
@@ -698,6 +795,35 @@ void trl_solve_params_default(trl_solve_params* p)
 }
 
 const char* trl_solver_last_error(void) { return g_err.c_str(); }
+
+int trl_solve_csr_minner_device(trl_cuda_handle h, const trl_solve_params* p, const trl_csr* op, const trl_csr* M, const double* X0, double* evals_host, double* evecs_dev,
+                                double* resid_host, trl_solve_info* info)
+{
+  try {
+    validate(p);
+    if (!h || !op || !M || !X0 || !evals_host || !info) throw std::invalid_argument("null argument");
+    if (p->mode != TRL_MODE_FP64) throw std::invalid_argument("the M inner product runs in FP64 only");
+    if (op->value_dtype != TRL_F64 || M->value_dtype != TRL_F64) throw std::invalid_argument("operator and M must have FP64 values");
+    if (M->n != op->n) throw std::invalid_argument("M must have the operator's size");
+    *info = trl_solve_info{};
+    auto ctx = Context::borrow(h);
+    ctx->set_batching(p->batching != 0);
+    return dispatch_minner(ctx, *p, op, M, X0, evals_host, evecs_dev, resid_host, info);
+  }
+  catch (const std::invalid_argument& e) {
+    return fail(e, TRL_EINVAL);
+  }
+  catch (const trl::cuda::out_of_device_memory& e) {
+    return fail(e, TRL_ENOMEM);
+  }
+  catch (const trl::cuda::device_timeout& e) {
+    return fail(e, TRL_ETIMEOUT);
+  }
+  catch (const std::exception& e) {
+    const std::string w = e.what();
+    return fail(e, w.find("Cholesky") != std::string::npos ? TRL_ECHOLESKY : (w.find("Eigendecomposition") != std::string::npos ? TRL_EEIGEN : TRL_ECUDA));
+  }
+}
 
 int trl_solve_csr_device(trl_cuda_handle h, const trl_solve_params* p, const trl_csr* A64, const trl_csr* A32, const double* X0, double* evals_host, double* evecs_dev,
                          double* resid_host, trl_solve_info* info)

@@ -41,6 +41,7 @@ CUDA_SYMBOLS = {
     "trl_cuda_launch_count": (C.c_uint64, [P]),
     "trl_cuda_inject_alloc_failures": (C.c_int, [P, C.c_int]),
     "trl_cuda_test_bounded_wait": (C.c_int, [P, C.c_uint]),
+    "trl_cuda_measure_dmma_rate": (C.c_int, [P, C.POINTER(C.c_double)]),
     "trl_cuda_malloc": (C.c_int, [P, C.POINTER(P), C.c_size_t]),
     "trl_cuda_free": (C.c_int, [P, P]),
     "trl_cuda_memcpy": (C.c_int, [P, P, P, C.c_size_t, C.c_int]),
@@ -114,6 +115,7 @@ SOLVER_SYMBOLS = {
     "trl_solve_params_default": (None, [C.POINTER(trl_solve_params)]),
     "trl_solve_csr_host": (C.c_int, [C.POINTER(trl_solve_params), C.c_int, I64, I64, P, P, P, P, P, P, P, C.POINTER(trl_solve_info)]),
     "trl_solve_csr_device": (C.c_int, [P, C.POINTER(trl_solve_params), P, P, P, P, P, P, C.POINTER(trl_solve_info)]),
+    "trl_solve_csr_minner_device": (C.c_int, [P, C.POINTER(trl_solve_params), P, P, P, P, P, P, C.POINTER(trl_solve_info)]),
     "trl_solver_last_error": (C.c_char_p, []),
     "trl_csr_read_mtx": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(C.POINTER(C.c_int32)),
                                    C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_double))]),
@@ -438,6 +440,23 @@ def solve_csr_device(handle: Handle, A64: DeviceCSRTensors, A32: DeviceCSRTensor
     L = solver_lib()
     st = L.trl_solve_csr_device(handle.h, C.byref(p), C.byref(A64.desc), None if A32 is None else C.byref(A32.desc), _ptr(X0),
                                 evals.ctypes.data, _ptr(evecs), resid.ctypes.data, C.byref(info))
+    if st != TRL_OK:
+        raise TrlError(st, L.trl_solver_last_error().decode())
+    out = _info_dict(info)
+    out.update(evals=evals, resid=resid)
+    return out
+
+
+def solve_csr_minner_device(handle: Handle, op: DeviceCSRTensors, M: DeviceCSRTensors, X0, evecs=None, **params) -> dict:
+    """Eigenpairs of an M-self-adjoint operator (e.g. M^{-1} K) with dot = V^T M W, through
+    trl_solve_csr_minner_device (FP64; X0: (n, bs) float64 CUDA tensor)."""
+    p = default_params(**params)
+    evals = np.zeros(p.nev)
+    resid = np.zeros(p.nev)
+    info = trl_solve_info()
+    L = solver_lib()
+    st = L.trl_solve_csr_minner_device(handle.h, C.byref(p), C.byref(op.desc), C.byref(M.desc), _ptr(X0), evals.ctypes.data, _ptr(evecs), resid.ctypes.data,
+                                       C.byref(info))
     if st != TRL_OK:
         raise TrlError(st, L.trl_solver_last_error().decode())
     out = _info_dict(info)

@@ -288,3 +288,26 @@ def initial_block(n: int, b: int, seed: int = 42) -> np.ndarray:
     ``initial_block()`` with std::mt19937(42) + normal_distribution, examples/openmp/csrtest.cc:94-96;
     the same values need not be reproduced — both backends receive this same array)."""
     return np.random.default_rng(seed).standard_normal((n, b))
+
+
+def diffusion2d_consistent_mass(m: int = 12, seed: int = 42, coupling: float = 0.05):
+    """K x = lambda M x on an m x m grid with a non-diagonal SPD mass: K as in
+    ``diffusion2d_mass``, M = diag(U[0.5, 1.5]) plus ``coupling`` between grid neighbours
+    (diagonally dominant for coupling < 1/8, hence SPD). Returns (K, M) as CSR."""
+    K, mass, edges = diffusion2d_mass(m, seed=seed)
+    a, b = edges["a"], edges["b"]
+    inner = b >= 0
+    n = m * m
+    d = np.arange(n, dtype=np.int64)
+    rows = np.concatenate([d, a[inner], b[inner]])
+    cols = np.concatenate([d, b[inner], a[inner]])
+    vals = np.concatenate([mass, np.full(int(inner.sum()), coupling), np.full(int(inner.sum()), coupling)])
+    return K, _from_coo(n, rows, cols, vals, kind="consistent_mass")
+
+
+def dense_csr(D: np.ndarray) -> CSRMatrix:
+    """A dense matrix as CSR with every entry stored."""
+    n = D.shape[0]
+    rows = np.repeat(np.arange(n, dtype=np.int64), n)
+    cols = np.tile(np.arange(n, dtype=np.int64), n)
+    return _from_coo(n, rows, cols, D.ravel(), kind="dense")
