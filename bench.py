@@ -12,13 +12,15 @@ The same JSON line carries the other workloads of the benchmark configurations, 
 once in FP64 and once in mixed precision after a short warm-up solve (`workloads`):
   elast64  3 dofs per node on a 64^3 node grid, 27-point coupling (n = 786,432, 61.7M
            entries), the 64 smallest eigenpairs through sigma*I - A, block size 8;
+  diff512  generalised K x = lambda M x on a 512^2 grid (log-normal edge conductivities,
+           lumped mass) as M^-1/2 K M^-1/2, the 16 smallest eigenpairs, block size 8;
   zipf4m   n = 4,194,304 random symmetric pattern with Zipf(1.5) row degrees capped at 512
            (145.5M entries), the 100 largest-magnitude eigenpairs, block sizes 4, 8, 16 with
            ncv = 32 * block size.
 Each also reports the prepared operator's SpMM GB/s (CUDA events, behind an L2 flush).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl trl|reference]
-                    [--workloads aniso96,elast64,zipf4m]
+                    [--workloads aniso96,elast64,diff512,zipf4m]
 
 --impl reference times the reference's own OpenMP implementation (the oracle built from the
 reference sources) on the host cores: one run of the reference BlockLanczos on the headline
@@ -65,13 +67,19 @@ def make_workload(name: str):
     if name == "zipf4m":
         A = P.zipf_symmetric(int(os.environ.get("TRL_BENCH_ZIPF_N", 4_194_304)), alpha=1.5, cap=512, seed=42)
         return A, 1.0, 0.0, f"zipf_symmetric n={A.n} nnz={A.nnz} (Zipf(1.5) degrees capped at 512, mirrored), 100 largest |lambda|, ncv=32*bs, tol=1e-10"
+    if name == "diff512":
+        K, mass, _ = P.diffusion2d_mass(512, sigma=1.0, seed=42)
+        A = P.scale_symmetric(K, 1.0 / np.sqrt(mass))
+        sigma = A.gershgorin_bound()
+        return A, -1.0, sigma, (f"generalised K x = lambda M x on a 512^2 grid (K: 5-point diffusion, log-normal(0,1) edge conductivities; M: lumped mass "
+                                f"U[0.5,1.5]) as M^-1/2 K M^-1/2, n={A.n} nnz={A.nnz}, 16 smallest via sigma*I - A, sigma = Gershgorin bound {sigma:.6f}, tol=1e-10")
     raise ValueError(name)
 
 
 REFINE_NAMES = {0: "lanczos", 1: "chebyshev", 2: "auto"}
 
 # solve shapes of the secondary workloads: (bs, nev, ncv)
-SHAPES = {"elast64": [(8, 64, 384)], "zipf4m": [(4, 100, 128), (8, 100, 256), (16, 100, 512)]}
+SHAPES = {"elast64": [(8, 64, 384)], "zipf4m": [(4, 100, 128), (8, 100, 256), (16, 100, 512)], "diff512": [(8, 16, 256)]}
 
 
 def peaks():
@@ -596,7 +604,7 @@ def profile_case(args):
     dt = torch.float32 if args.fp32 else torch.float64
     h = native.Handle(0)
     if args.case in ("solve", "mixed", "solves"):
-        nev, ncv = {"aniso96": (CFG["nev"], CFG["ncv"]), "elast64": (64, 384), "zipf4m": (100, 32 * bs)}[args.workload]
+        nev, ncv = {"aniso96": (CFG["nev"], CFG["ncv"]), "elast64": (64, 384), "zipf4m": (100, 32 * bs), "diff512": (16, 32 * bs)}[args.workload]
         S = GpuSolver(h, A, alpha, beta, bs, nev, ncv)
         S.common["fp32_tol"] = args.fp32_tol
         if args.case == "solve":
@@ -725,12 +733,12 @@ def main():
     ap.add_argument("--impl", choices=["trl", "reference"], default="trl")
     ap.add_argument("--fp32-tol", type=float, default=3e-3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workloads", default="aniso96,elast64,zipf4m", help="headline workload plus the secondary ones solved once per mode")
+    ap.add_argument("--workloads", default="aniso96,elast64,diff512,zipf4m", help="headline workload plus the secondary ones solved once per mode")
     ap.add_argument("--secondary-modes", default="fp64,mixed")
     ap.add_argument("--cpu-cycles", type=int, default=0, help=argparse.SUPPRESS)  # child process of the CPU legs
     ap.add_argument("--case", choices=["solve", "mixed", "solves", "spmm", "spmm-csr", "spmm-rates", "dot", "update", "project", "rotate", "small-eigen", "dmma-peak"],
                     default=None, help="profiling driver: run one piece of a workload and exit (see profile_case)")
-    ap.add_argument("--workload", default="aniso96", choices=["aniso96", "elast64", "zipf4m"])
+    ap.add_argument("--workload", default="aniso96", choices=["aniso96", "elast64", "zipf4m", "diff512"])
     ap.add_argument("--modes", default="fp64,mixed")
     ap.add_argument("--params", default="{}", help="solves: extra solver parameters (JSON object of trl_solve_params fields)")
     ap.add_argument("--bs", type=int, default=8)

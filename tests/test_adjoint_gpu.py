@@ -185,3 +185,68 @@ def test_autograd_function_through_the_gpu_solver(cuda_handle):
     dk_ref, dm_ref = grad_from_vectors(cuda_handle, K, mass, edges, X_ref, lam_ref, w)
     assert np.max(np.abs(kappa.grad.numpy() - dk_ref)) < 1e-6 * np.abs(dk_ref).max()
     assert np.max(np.abs(mt.grad.numpy() - dm_ref)) < 1e-6 * np.abs(dm_ref).max()
+
+
+def _identity_difference(K, mass, edges, which, idx, h, Xp, Xm, lam_m):
+    """lambda_+ - lambda_- for every pair from the eigenvectors of the two perturbed problems,
+    through the exact identities (K symmetric, x_+ and x_- exact eigenvectors):
+      edge e (kappa_e scaled by 1 +- h):  (lambda_+ - lambda_-) x_+^T M x_- = x_-^T (K_+ - K_-) x_+
+                                          = 2 h kappa_e (x_+[a] - x_+[b]) (x_-[a] - x_-[b]);
+      mass i (m_i scaled by 1 +- h):      (lambda_+ - lambda_-) x_-^T M_+ x_+ = -lambda_- x_+^T (M_+ - M_-) x_-
+                                          = -lambda_- 2 h m_i x_+[i] x_-[i].
+    They give the difference of the two solves' eigenvalues without the cancellation of
+    subtracting two nearly equal numbers (the smallest eigenvalues are ~1e-6 of the operator's
+    norm here)."""
+    if which == "edge":
+        a, b = edges["a"][idx], edges["b"][idx]
+        dp = Xp[a] - (Xp[b] if b >= 0 else 0.0)
+        dm = Xm[a] - (Xm[b] if b >= 0 else 0.0)
+        return 2 * h * edges["kappa"][idx] * dp * dm / np.einsum("ic,i,ic->c", Xp, mass, Xm)
+    mp = mass.copy()
+    mp[idx] *= 1 + h
+    return -lam_m * 2 * h * mass[idx] * Xp[idx] * Xm[idx] / np.einsum("ic,i,ic->c", Xm, mp, Xp)
+
+
+@pytest.mark.slow
+def test_full_size_gradient_against_finite_differences(cuda_handle):
+    """The 512 x 512 generalised problem (n = 262,144): the 16 smallest eigenpairs by the
+    mixed-precision solver to 1e-12, the adjoint gradient of f = sum w_c lambda_c over every edge
+    conductivity and mass, and central finite differences (relative step 1e-3) on 50 random
+    entries (25 edges, 25 masses), each from two perturbed GPU solves."""
+    K, mass, edges = P.diffusion2d_mass(512, sigma=1.0, seed=42)
+    k, bs, ncv, tol, hstep = 16, 8, 256, 1e-12, 1e-3
+    w = np.random.default_rng(7).uniform(size=k)
+    X0 = P.initial_block(K.n, bs, seed=42)
+    mode = native.TRL_MODE_MIXED
+
+    def solve(Kx, mx):
+        lam, X, out = G.solve_smallest(cuda_handle, Kx, mx, k, bs, ncv, X0, tol=tol, mode=mode)
+        assert out["converged"] and out["max_theta_residual"] < 10 * tol
+        order = np.argsort(lam)
+        return lam[order], X[:, order].cpu().numpy()
+
+    lam, X = solve(K, mass)
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    dk, dm = G.eigen_sum_gradient(cuda_handle, K, K.n, edges, Xd, lam, w)
+    rng = np.random.default_rng(11)
+    picks = [("edge", int(i)) for i in rng.choice(edges["a"].size, 25, replace=False)] + [("mass", int(i)) for i in rng.choice(K.n, 25, replace=False)]
+    errs = []
+    for which, idx in picks:
+        res = []
+        for s in (+1, -1):
+            if which == "edge":
+                kap = edges["kappa"].copy()
+                kap[idx] *= 1 + s * hstep
+                res.append(solve(P.assemble_diffusion(K.n, edges["a"], edges["b"], kap), mass))
+            else:
+                mm = mass.copy()
+                mm[idx] *= 1 + s * hstep
+                res.append(solve(K, mm))
+        (lp, Xp), (lm, Xm) = res
+        d = _identity_difference(K, mass, edges, which, idx, hstep, Xp, Xm, lm)
+        p = edges["kappa"][idx] if which == "edge" else mass[idx]
+        fd = float(np.dot(w, d)) / (2 * hstep * p)
+        adj = dk[idx] if which == "edge" else dm[idx]
+        errs.append(abs(fd - adj) / max(abs(adj), 1e-300))
+    print("full-size FD agreement: max rel err %.2e, median %.2e" % (max(errs), float(np.median(errs))))
+    assert max(errs) < 1e-6, sorted(errs)[-5:]
