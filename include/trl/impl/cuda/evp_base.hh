@@ -235,7 +235,10 @@ public:
   /// (trl_cuda_project_out_sketch): projects only when the random sketch S of those blocks
   /// shows a loss of orthogonality above set_partial_threshold() (default 1e-12). S is kept
   /// here: extended by the blocks added since the last call, rebuilt when the basis changed
-  /// (a restart rotates it into the other multivector, or count went down). With
+  /// (a restart rotates it into the other multivector, or count went down). The sketch
+  /// assumes the basis is append-only between those events: a caller that rewrites blocks
+  /// already sketched in place (same V0, count not decreasing) calls reset_sketch() first.
+  /// The reference driver never does; its restarts swap V and W. With
   /// set_partial_pairs (the default) a step whose test fired also projects the next step:
   /// projected alone, a step leaves the loss of its unprojected predecessor to return two
   /// steps later through the recurrence's B term.
@@ -288,6 +291,14 @@ public:
   double partial_threshold() const { return partial_threshold_; }
   void set_partial_pairs(bool on) { partial_pairs_ = on; }
   bool partial_pairs() const { return partial_pairs_; }
+  /// Forget the partial reorthogonalisation's sketch and its pending pair: the next
+  /// project_out_sketch rebuilds S from the blocks it is given.
+  void reset_sketch()
+  {
+    sketch_v0_ = nullptr;
+    sketch_count_ = 0;
+    if (sketch_pair_.get()) ctx_->check(trl_cuda_memset_zero(ctx_->handle(), sketch_pair_.get(), sizeof(int)), "sketch pair state");
+  }
 
   Context& context() const { return *ctx_; }
   const std::shared_ptr<Context>& shared_context() const { return ctx_; }

@@ -37,12 +37,13 @@ enum trl_mode { TRL_MODE_FP64 = 0, TRL_MODE_FP32 = 1, TRL_MODE_MIXED = 2 };
 /* Reorthogonalisation strategy: the reference's ModifiedGS, or the backend's block classical
  * Gram-Schmidt variants (include/trl/impl/cuda/reorthogonalization.hh). */
 enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEEDED = 2, TRL_REORTH_CGS1 = 3, TRL_REORTH_PARTIAL = 4 };
-/* FP64 refinement of the mixed mode. */
 /* FP64 refinement of the mixed mode. TRL_REFINE_AUTO (default): the Chebyshev refinement
  * after its first Rayleigh-Ritz step predicts its own time (degrees to the tolerance at the
- * predicted rate x one measured multi-block SpMM) and hands over to the Lanczos refinement
- * when that is predicted cheaper (estimated from the FP32 phase's time and the orders of
- * magnitude left). */
+ * predicted rate x one measured multi-block SpMM and a share of one measured
+ * re-orthonormalisation; a two-sided filter, for kept values on both sides of zero, with a
+ * 4x margin) and hands over to the Lanczos refinement when that is predicted cheaper
+ * (estimated from the FP32 phase's time and the orders of magnitude left), or later, at the
+ * start of a round, once the filter has taken three times that estimate. */
 enum trl_refine { TRL_REFINE_LANCZOS = 0, TRL_REFINE_CHEBYSHEV = 1, TRL_REFINE_AUTO = 2 };
 
 typedef struct trl_solve_params {
@@ -87,9 +88,10 @@ typedef struct trl_solve_info {
   double op_norm1;          /* ||op||_1 = max row sum of |alpha*A + beta*I| */
   unsigned long long kernel_launches; /* kernels launched by the backend during the call */
   double h2d_bytes, d2h_bytes;        /* host<->device traffic of the call */
-  unsigned refine_rounds;   /* TRL_REFINE_CHEBYSHEV: Rayleigh-Ritz rounds (0: not used) */
-  unsigned refine_degree;   /* TRL_REFINE_CHEBYSHEV: total filter degree */
-  unsigned refine_degree_fp32; /* TRL_REFINE_CHEBYSHEV: of which applied in FP32 */
+  unsigned refine_rounds;   /* Chebyshev refinement: Rayleigh-Ritz rounds (0: not run; also
+                               counted when it handed over to the Lanczos refinement) */
+  unsigned refine_degree;   /* Chebyshev refinement: total filter degree */
+  unsigned refine_degree_fp32; /* Chebyshev refinement: of which applied in FP32 */
   int refine_used;              /* TRL_MODE_MIXED: the refinement that ran (trl_refine) */
   double refine_predicted_s;    /* TRL_REFINE_AUTO: the Chebyshev refinement's predicted time */
   double refine_lanczos_estimate_s; /* TRL_REFINE_AUTO: the Lanczos refinement's estimated time */

@@ -55,7 +55,11 @@ def test_dot_matches_reference(cuda_handle, oracle, bs, dtype, n):
 @pytest.mark.parametrize("bs", BS)
 @pytest.mark.parametrize("dtype", DT)
 @pytest.mark.parametrize("nblk", [1, 3, 9, 17, 49])
-def test_multiblock_dot_and_update(cuda_handle, bs, dtype, nblk):
+def test_multiblock_dot_and_update(cuda_handle, oracle, bs, dtype, nblk):
+    """One classical Gram-Schmidt pass against nblk blocks, C_j = V_j^T w then
+    w -= sum_j V_j C_j, against the reference's BlockView::dot and subtract_product applied
+    block by block (blockview.hh:152-182, 189-201), the loop of the reference's
+    orthogonalisation strategies."""
     rng = np.random.default_rng(nblk * 7 + bs)
     n = 4099
     V = as_dt(rng.standard_normal((nblk, n, bs)), dtype)
@@ -63,11 +67,15 @@ def test_multiblock_dot_and_update(cuda_handle, bs, dtype, nblk):
     Cd = torch.zeros((nblk, bs, bs), dtype=torch.float64, device="cuda")
     Vd, wd = dev(V, dtype), dev(w, dtype)
     cuda_handle.block_dot(Vd, wd, Cd)
-    Cref = np.einsum("jnb,nc->jbc", V, w)
+    Cref = np.zeros((nblk, bs, bs))
+    for j in range(nblk):
+        oracle.block_view_op(bs, oracle.OP_DOT, V[j].copy(), w.copy(), Cref[j])
     close(host(Cd), Cref, np.einsum("jnb,nc->jbc", np.abs(V), np.abs(w)).max())
-    # W -= sum_j V_j C_j  (one classical Gram-Schmidt pass)
     cuda_handle.block_update(wd, Vd, Cd)
-    ref = w - np.einsum("jnb,jbc->nc", V, host(Cd))
+    C = host(Cd)
+    ref = w.copy()
+    for j in range(nblk):
+        oracle.block_view_op(bs, oracle.OP_SUB_PROD, ref, V[j].copy(), C[j].copy())
     got = host(wd)
     tol = 1e-12 if dtype == torch.float64 else 2e-7
     close(got, ref, np.abs(ref).max() + np.abs(w).max(), tol)

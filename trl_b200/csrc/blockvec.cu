@@ -51,6 +51,7 @@ __device__ __forceinline__ void vsub<float>(float4& a, const float4& b)
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_sub(T* __restrict__ X, const T* __restrict__ Y, int64_t count, int vec_ok)
 {
+  ::trl_detail::pdl_enter();
   const int64_t tid = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   using V = typename Vec16<T>::type;
@@ -73,6 +74,7 @@ __global__ void __launch_bounds__(kThreads) k_sub(T* __restrict__ X, const T* __
 template <typename D, typename S>
 __global__ void __launch_bounds__(kThreads) k_convert(D* __restrict__ dst, const S* __restrict__ src, int64_t count)
 {
+  ::trl_detail::pdl_enter();
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += stride) dst[i] = static_cast<D>(src[i]);
 }
@@ -88,6 +90,7 @@ template <typename T, int BS, int JC, int G>
 __global__ void __launch_bounds__(kThreads) k_block_dot(const T* __restrict__ V, int64_t vstride, int nblk, const T* __restrict__ W, int64_t n, int64_t rows_per_cta,
                                                         double* __restrict__ partial, const int* __restrict__ cond = nullptr)
 {
+  ::trl_detail::pdl_enter();
   if (cond && *cond == 0) return; // device-side skip (uniform over the grid)
   constexpr int NT = (BS + 7) / 8;
   constexpr int BB = BS * BS;
@@ -189,6 +192,7 @@ template <typename T, int BS, int JC, int S, int TB>
 __global__ void __launch_bounds__(kThreads) k_block_dot_bulk(const T* __restrict__ V, int64_t vstride, int nblk, const T* __restrict__ W, int64_t n, int64_t rows_per_cta,
                                                              double* __restrict__ partial, int* status, const int* __restrict__ cond)
 {
+  ::trl_detail::pdl_enter();
   if (cond && *cond == 0) return; // device-side skip (uniform over the grid)
   constexpr int NT = (BS + 7) / 8;
   constexpr int BB = BS * BS;
@@ -338,6 +342,7 @@ constexpr int kRedThreads = 1024;
 __global__ void __launch_bounds__(kRedThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out,
                                                                  const int* __restrict__ cond = nullptr)
 {
+  ::trl_detail::pdl_enter();
   if (cond && *cond == 0) return;
   constexpr int SL = kRedThreads / 32;
   __shared__ double part[SL][33];
@@ -366,6 +371,7 @@ template <typename T, int BS, int NBMAX, int RT, int U>
 __global__ void __launch_bounds__(kThreads) k_block_gemm(const T* in, int64_t istride, int MB, const double* __restrict__ coef, int ldc, int transpose_coef, T* out,
                                                          int64_t ostride, int NB, int64_t n, int accumulate, double sign)
 {
+  ::trl_detail::pdl_enter();
   constexpr int NT = (BS + 7) / 8;
   constexpr int KS = (BS + 3) / 4;
   const int lane = threadIdx.x & 31;
@@ -461,6 +467,7 @@ template <typename T, int BS, int NTC, int RT, int D>
 __global__ void __launch_bounds__(kRotThreads, 1) k_rotate(const T* __restrict__ V, int64_t vstride, int m, const double* __restrict__ Y, int ldy, int N, int c0,
                                                            T* __restrict__ W, int64_t wstride, int64_t n)
 {
+  ::trl_detail::pdl_enter();
   constexpr int KSB = BS / 4; // k-steps per input block
   extern __shared__ double sY[];
   const int ks_total = m * KSB;
@@ -583,6 +590,7 @@ template <typename T, int BS, int RT, int U>
 __global__ void __launch_bounds__(kThreads) k_update_gram(const T* in, int64_t istride, int MB, const double* __restrict__ coef, T* out, int64_t n, int accumulate, double sign,
                                                           double* __restrict__ gram_partial, const int* __restrict__ cond)
 {
+  ::trl_detail::pdl_enter();
   if (cond && *cond == 0) return;
   constexpr int NT = (BS + 7) / 8;
   constexpr int KS = (BS + 3) / 4;
@@ -702,6 +710,7 @@ __global__ void __launch_bounds__(kThreads) k_update_gram(const T* in, int64_t i
 template <int BS>
 __global__ void k_dgks_flag(const double* __restrict__ G_before, const double* __restrict__ G_after, double eta2, int* __restrict__ flag)
 {
+  ::trl_detail::pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   int f = 0;
   for (int c = 0; c < BS; ++c) f |= (G_after[c * BS + c] < eta2 * G_before[c * BS + c]);
@@ -714,6 +723,7 @@ __global__ void k_dgks_flag(const double* __restrict__ G_before, const double* _
 template <int BS>
 __global__ void k_sketch_flag(const double* __restrict__ E, const double* __restrict__ G, double thr2, int* __restrict__ flag, int* __restrict__ pair)
 {
+  ::trl_detail::pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double e2 = 0.0, tr = 0.0;
   for (int i = 0; i < BS * BS; ++i) e2 = fma(E[i], E[i], e2);
@@ -731,6 +741,7 @@ __global__ void k_sketch_flag(const double* __restrict__ E, const double* __rest
 template <int BS>
 __global__ void k_dgks_flag_after(const int* __restrict__ flag1, const double* __restrict__ G_before, const double* __restrict__ G_after, double eta2, int* __restrict__ flag2)
 {
+  ::trl_detail::pdl_enter();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   int f = 0;
   if (*flag1)
@@ -742,6 +753,7 @@ __global__ void k_dgks_flag_after(const int* __restrict__ flag1, const double* _
 __global__ void k_select_block3(const int* __restrict__ f1, const int* __restrict__ f2, const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ c,
                                 double* __restrict__ dst, int count)
 {
+  ::trl_detail::pdl_enter();
   const int e = threadIdx.x;
   if (e < count) dst[e] = *f2 ? c[e] : (*f1 ? b[e] : a[e]);
 }
@@ -749,6 +761,7 @@ __global__ void k_select_block3(const int* __restrict__ f1, const int* __restric
 // dst = *flag ? a : b  (BS x BS)
 __global__ void k_select_block(const int* __restrict__ flag, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ dst, int count)
 {
+  ::trl_detail::pdl_enter();
   const int e = threadIdx.x;
   if (e < count) dst[e] = *flag ? a[e] : b[e];
 }
@@ -763,6 +776,7 @@ template <int BS>
 __global__ void __launch_bounds__(kRedThreads) k_gram_factor(const double* __restrict__ src, int chunks, double* __restrict__ Uinv, double* __restrict__ R, int first,
                                                              int* status)
 {
+  ::trl_detail::pdl_enter();
   constexpr int SL = kRedThreads / 32; // slices of the chunk range per output
   __shared__ double G[BS * BS], L[BS][BS + 1], Li[BS][BS + 1], Ro[BS * BS];
   __shared__ double part[SL][33];
@@ -871,10 +885,10 @@ int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, i
   double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
   if (!partial) return TRL_ENOMEM;
   dim3 grid(gj, static_cast<unsigned>(chunks));
-  k_block_dot<T, BS, JC, G><<<grid, kThreads, 0, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial, cond);
+  launch(k_block_dot<T, BS, JC, G>, grid, kThreads, 0, h->stream, V, n * BS, nblk, W, n, rows_per_cta, partial, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
+  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream, partial, static_cast<int>(chunks), len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -896,10 +910,10 @@ int launch_block_dot_two(trl_cuda_context* h, const T* A, const T* B, const T* W
   double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
   if (!partial) return TRL_ENOMEM;
   const int64_t vstride = B - A; // elements between the two blocks
-  k_block_dot<T, BS, JC, G><<<dim3(1, static_cast<unsigned>(chunks)), kThreads, 0, h->stream>>>(A, vstride, 2, W, n, rows_per_cta, partial, nullptr);
+  launch(k_block_dot<T, BS, JC, G>, dim3(1, static_cast<unsigned>(chunks)), kThreads, 0, h->stream, A, vstride, 2, W, n, rows_per_cta, partial, nullptr);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, nullptr);
+  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream, partial, static_cast<int>(chunks), len, C, nullptr);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -929,10 +943,10 @@ int launch_block_dot_bulk(trl_cuda_context* h, const T* V, int nblk, const T* W,
   chunks = (n + rows_per_cta - 1) / rows_per_cta;
   double* partial = static_cast<double*>(workspace(h, static_cast<size_t>(chunks) * len * sizeof(double)));
   if (!partial) return TRL_ENOMEM;
-  k_block_dot_bulk<T, BS, JC, S, TB><<<dim3(gj, static_cast<unsigned>(chunks)), kThreads, smem, h->stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial, h->d_status, cond);
+  launch(k_block_dot_bulk<T, BS, JC, S, TB>, dim3(gj, static_cast<unsigned>(chunks)), kThreads, smem, h->stream, V, n * BS, nblk, W, n, rows_per_cta, partial, h->d_status, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream>>>(partial, static_cast<int>(chunks), len, C, cond);
+  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream, partial, static_cast<int>(chunks), len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -991,7 +1005,7 @@ int launch_update_gram_partials(trl_cuda_context* h, const T* in, int MB, const 
   *partial = static_cast<double*>(workspace(h, static_cast<size_t>(grid) * BS * BS * sizeof(double)));
   *chunks = static_cast<int>(grid);
   if (!*partial) return TRL_ENOMEM;
-  k_update_gram<T, BS, RT, 1><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
+  launch(k_update_gram<T, BS, RT, 1>, grid, kThreads, 0, h->stream, in, n * BS, MB, coef, out, n, accumulate, sign, *partial, cond);
   return after_launch(h, "update_gram");
 }
 
@@ -1002,7 +1016,7 @@ int launch_update_gram(trl_cuda_context* h, const T* in, int MB, const double* c
   int chunks = 0;
   int st = launch_update_gram_partials<T, BS>(h, in, MB, coef, out, n, accumulate, sign, cond, &partial, &chunks);
   if (st) return st;
-  k_reduce_partials<<<(BS * BS + 31) / 32, kRedThreads, 0, h->stream>>>(partial, chunks, BS * BS, G, cond);
+  launch(k_reduce_partials, (BS * BS + 31) / 32, kRedThreads, 0, h->stream, partial, chunks, BS * BS, G, cond);
   return after_launch(h, "update_gram reduce");
 }
 
@@ -1015,9 +1029,9 @@ void launch_gemm_nb(trl_cuda_context* h, const T* in, int MB, const double* coef
   constexpr int U = (KS >= 4) ? 2 : 4;
   const unsigned grid = grid_for(h, (n + 8 * RT - 1) / (8 * RT), kWarps, 8);
   if (MB == 1) // a single input block: no point loading it U times
-    k_block_gemm<T, BS, NBMAX, RT, 1><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
+    launch(k_block_gemm<T, BS, NBMAX, RT, 1>, grid, kThreads, 0, h->stream, in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
   else
-    k_block_gemm<T, BS, NBMAX, RT, U><<<grid, kThreads, 0, h->stream>>>(in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
+    launch(k_block_gemm<T, BS, NBMAX, RT, U>, grid, kThreads, 0, h->stream, in, n * BS, MB, coef, ldc, transpose, out, n * BS, nb, n, accumulate, sign);
 }
 
 template <typename T, int BS>
@@ -1063,7 +1077,7 @@ int launch_rotate_chunk(trl_cuda_context* h, const T* V, int m, const double* Y,
   const int64_t need = (tiles + kRotThreads / 32 - 1) / (kRotThreads / 32);
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  kern<<<static_cast<unsigned>(grid), kRotThreads, smem, h->stream>>>(V, n * BS, m, Y, ldy, N, c0, W, n * BS, n);
+  launch(kern, static_cast<unsigned>(grid), kRotThreads, smem, h->stream, V, n * BS, m, Y, ldy, N, c0, W, n * BS, n);
   return after_launch(h, "rotate");
 }
 
@@ -1142,7 +1156,7 @@ int trl_cuda_bv_sub(trl_cuda_handle h, int dtype, void* X, const void* Y, int64_
   ProfScope prof(h, PROF_SUB, 3.0 * count * elt_size(dtype));
   const int vec_ok = ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 15) == 0;
   const unsigned grid = grid_for(h, count / 4 + 1, kThreads, 8);
-  TRL_DISPATCH_DT(dtype, k_sub<T><<<grid, kThreads, 0, h->stream>>>(static_cast<T*>(X), static_cast<const T*>(Y), count, vec_ok));
+  TRL_DISPATCH_DT(dtype, launch(k_sub<T>, grid, kThreads, 0, h->stream, static_cast<T*>(X), static_cast<const T*>(Y), count, vec_ok));
   return after_launch(h, "bv_sub");
 }
 
@@ -1157,9 +1171,9 @@ int trl_cuda_convert(trl_cuda_handle h, int dst_dtype, void* dst, int src_dtype,
   if (dst_dtype == src_dtype) return trl_cuda_memcpy(h, dst, src, static_cast<size_t>(count) * elt_size(dst_dtype), TRL_D2D);
   const unsigned grid = grid_for(h, count, kThreads * 4, 8);
   if (dst_dtype == TRL_F64)
-    k_convert<double, float><<<grid, kThreads, 0, h->stream>>>(static_cast<double*>(dst), static_cast<const float*>(src), count);
+    launch(k_convert<double, float>, grid, kThreads, 0, h->stream, static_cast<double*>(dst), static_cast<const float*>(src), count);
   else
-    k_convert<float, double><<<grid, kThreads, 0, h->stream>>>(static_cast<float*>(dst), static_cast<const double*>(src), count);
+    launch(k_convert<float, double>, grid, kThreads, 0, h->stream, static_cast<float*>(dst), static_cast<const double*>(src), count);
   return after_launch(h, "convert");
 }
 
@@ -1275,7 +1289,7 @@ int trl_cuda_cholqr_gram(trl_cuda_handle h, int dtype, void* X, int64_t n, int b
   int chunks = 0;
   for (int p = 0; p < passes; ++p) {
     int st = TRL_OK;
-    TRL_DISPATCH_BS(bs, k_gram_factor<BS><<<1, kRedThreads, 0, h->stream>>>(src, chunks, Uinv, R, p == 0, h->d_status));
+    TRL_DISPATCH_BS(bs, launch(k_gram_factor<BS>, 1, kRedThreads, 0, h->stream, src, chunks, Uinv, R, p == 0, h->d_status));
     st = after_launch(h, "cholqr factor");
     if (st) return st;
     if (p + 1 < passes) {
@@ -1338,7 +1352,7 @@ int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, 
       cudaMemsetAsync(flag, 0x01, sizeof(int), h->stream);
     }
     else {
-      k_dgks_flag<BS><<<1, 32, 0, h->stream>>>(Gw0, Gw1, eta * eta, flag);
+      launch(k_dgks_flag<BS>, 1, 32, 0, h->stream, Gw0, Gw1, eta * eta, flag);
       if ((st = after_launch(h, "dgks"))) return st;
     }
     // pass 2, only where the flag is set (decided on the device; its bytes are not credited
@@ -1349,7 +1363,7 @@ int trl_cuda_project_out(trl_cuda_handle h, int dtype, const void* V, int nblk, 
       if (!st) st = launch_update_gram<T, BS>(h, Vt, nblk, C2, Wt, n, 1, -1.0, Gw2, flag);
     }
     if (st) return st;
-    k_select_block<<<1, 256, 0, h->stream>>>(flag, Gw2, Gw1, G, BB);
+    launch(k_select_block, 1, 256, 0, h->stream, flag, Gw2, Gw1, G, BB);
     st = after_launch(h, "select");
   }));
   return st;
@@ -1386,7 +1400,7 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
       st = launch_block_dot_two<T, BS>(h, St, Wt, Wt, n, E);
     }
     if (st) return st;
-    k_sketch_flag<BS><<<1, 32, 0, h->stream>>>(E, Gw0, thr * thr, flag1, pair_state);
+    launch(k_sketch_flag<BS>, 1, 32, 0, h->stream, E, Gw0, thr * thr, flag1, pair_state);
     if ((st = after_launch(h, "sketch flag"))) return st;
     // both passes only where flagged (decided on the device; their bytes are not credited
     // to the profile because the host does not know whether they ran)
@@ -1395,13 +1409,13 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
       st = launch_block_dot<T, BS>(h, Vt, nblk, Wt, n, C1, flag1);
       if (!st) st = launch_update_gram<T, BS>(h, Vt, nblk, C1, Wt, n, 1, -1.0, Gw1, flag1);
       if (st) return st;
-      k_dgks_flag_after<BS><<<1, 32, 0, h->stream>>>(flag1, Gw0, Gw1, eta * eta, flag2);
+      launch(k_dgks_flag_after<BS>, 1, 32, 0, h->stream, flag1, Gw0, Gw1, eta * eta, flag2);
       if ((st = after_launch(h, "dgks"))) return st;
       st = launch_block_dot<T, BS>(h, Vt, nblk, Wt, n, C2, flag2);
       if (!st) st = launch_update_gram<T, BS>(h, Vt, nblk, C2, Wt, n, 1, -1.0, Gw2, flag2);
     }
     if (st) return st;
-    k_select_block3<<<1, 256, 0, h->stream>>>(flag1, flag2, Gw0, Gw1, Gw2, G, BB);
+    launch(k_select_block3, 1, 256, 0, h->stream, flag1, flag2, Gw0, Gw1, Gw2, G, BB);
     st = after_launch(h, "select");
 #ifdef TRL_DEBUG_TRACE
     // debug builds (-DTRL_DEBUG_TRACE) with TRL_PARTIAL_TRACE set: one stderr line per call
@@ -1428,6 +1442,7 @@ int trl_cuda_project_out_sketch(trl_cuda_handle h, int dtype, const void* V, int
 namespace {
 __global__ void __launch_bounds__(kThreads) k_unblock(const double* __restrict__ X, int64_t n, int bs, int ncols, double* __restrict__ out)
 {
+  ::trl_detail::pdl_enter();
   const int64_t total = n * ncols;
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += stride) {
@@ -1445,7 +1460,7 @@ extern "C" int trl_cuda_unblock(trl_cuda_handle h, const double* X, int64_t n, i
   if (n == 0 || ncols == 0) return TRL_OK;
   if (!X || !out) return set_error(h, TRL_EINVAL, "null pointer");
   ProfScope prof(h, PROF_COPY, 16.0 * n * ncols);
-  k_unblock<<<grid_for(h, n * ncols, kThreads * 4, 8), kThreads, 0, h->stream>>>(X, n, bs, ncols, out);
+  launch(k_unblock, grid_for(h, n * ncols, kThreads * 4, 8), kThreads, 0, h->stream, X, n, bs, ncols, out);
   return after_launch(h, "unblock");
 }
 
@@ -1505,9 +1520,9 @@ static int noalloc_dot(cudaStream_t stream, int sms, double* partial, const T* V
   chunks = (n + rows_per_cta - 1) / rows_per_cta;
   // every (chunk, block) entry of the partials is written before it is read in this call,
   // so nothing left in the array by an earlier call is used and nothing needs clearing
-  k_block_dot<T, BS, JC, G><<<dim3(gj, static_cast<unsigned>(chunks)), kThreads, 0, stream>>>(V, n * BS, nblk, W, n, rows_per_cta, partial);
+  launch(k_block_dot<T, BS, JC, G>, dim3(gj, static_cast<unsigned>(chunks)), kThreads, 0, stream, V, n * BS, nblk, W, n, rows_per_cta, partial, nullptr);
   if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
-  k_reduce_partials<<<static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, stream>>>(partial, static_cast<int>(chunks), len, C);
+  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, stream, partial, static_cast<int>(chunks), len, C, nullptr);
   if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
   return TRL_OK;
 }
@@ -1551,6 +1566,7 @@ constexpr int kDmmaChains = 8;
 
 __global__ void __launch_bounds__(256) k_dmma_rate(int iters, double* __restrict__ out)
 {
+  ::trl_detail::pdl_enter();
   double d0[kDmmaChains], d1[kDmmaChains];
   const double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * blockIdx.x;
 #pragma unroll
@@ -1577,9 +1593,9 @@ extern "C" int trl_cuda_measure_dmma_rate(trl_cuda_handle h, double* host_tflops
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
-  k_dmma_rate<<<grid, 256, 0, h->stream>>>(iters, out); // warm-up
+  launch(k_dmma_rate, grid, 256, 0, h->stream, iters, out); // warm-up
   cudaEventRecord(a, h->stream);
-  k_dmma_rate<<<grid, 256, 0, h->stream>>>(iters, out);
+  launch(k_dmma_rate, grid, 256, 0, h->stream, iters, out);
   cudaEventRecord(b, h->stream);
   const cudaError_t e = cudaEventSynchronize(b);
   float ms = 0.f;

@@ -122,6 +122,44 @@ inline unsigned grid_for(const trl_cuda_context* h, int64_t work_items, int item
   return static_cast<unsigned>(need < cap ? need : cap);
 }
 
+// Programmatic dependent launch. Every kernel of the library starts with pdl_enter(). A
+// kernel launched by launch() below (programmatic stream serialization) may have its CTAs
+// scheduled while the previous kernel of its stream is still finishing; they wait in
+// griddepcontrol.wait until that kernel has completed and its memory operations are
+// visible, before touching any global memory, so the ordering is that of a plain launch
+// while the launch latency of a chain of short dependent kernels overlaps the tail of
+// each predecessor. The trigger that follows lets this kernel's own successor be
+// scheduled once all of its CTAs have passed the wait. For a kernel launched without the
+// attribute both instructions return at once.
+__device__ __forceinline__ void pdl_enter()
+{
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// true unless the environment sets TRL_PDL=0 (read once per process)
+bool pdl_enabled();
+
+// kernel<<<grid, block, smem, stream>>>(args...) with programmatic stream serialization
+// when pdl_enabled() and the stream is not the legacy default stream (whose implicit
+// synchronisation with other streams is left as it is). Every kernel parameter is passed
+// explicitly (no default arguments).
+template <typename... P, typename... A>
+cudaError_t launch(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, A&&... args)
+{
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = (pdl_enabled() && stream != nullptr && stream != cudaStreamLegacy) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 } // namespace trl_detail
 
 // FP64 tensor-core MMA, m8n8k4 (DMMA). Fragment layout (PTX ISA, mma.m8n8k4 .f64):

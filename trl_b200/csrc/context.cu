@@ -2,6 +2,7 @@
 #include "common.cuh"
 
 #include <cstdarg>
+#include <cstdlib>
 #include <new>
 
 namespace trl_detail {
@@ -17,6 +18,15 @@ int set_error(trl_cuda_context* h, int status, const char* fmt, ...)
     h->last_error = buf;
   }
   return status;
+}
+
+bool pdl_enabled()
+{
+  static const bool on = [] {
+    const char* v = std::getenv("TRL_PDL");
+    return !(v && v[0] == '0');
+  }();
+  return on;
 }
 
 int after_launch(trl_cuda_context* h, const char* what)
@@ -343,6 +353,7 @@ namespace {
 // phase never completes, the wait gives up after `polls` polls and records TRL_DEV_TIMEOUT.
 __global__ void k_wait_never_completes(int* status, unsigned polls)
 {
+  ::trl_detail::pdl_enter();
   __shared__ uint64_t bar;
   if (threadIdx.x != 0) return;
   mbar_init(&bar, 2);
@@ -364,6 +375,6 @@ extern "C" int trl_cuda_test_bounded_wait(trl_cuda_handle h, unsigned polls)
 {
   TRL_CHECK_HANDLE(h);
   if (polls == 0 || polls > (1u << 24)) return set_error(h, TRL_EINVAL, "polls must be in [1, 2^24]");
-  k_wait_never_completes<<<1, 32, 0, h->stream>>>(h->d_status, polls);
+  launch(k_wait_never_completes, 1, 32, 0, h->stream, h->d_status, polls);
   return after_launch(h, "bounded wait");
 }

@@ -99,6 +99,7 @@ __device__ __forceinline__ int sort_key(int64_t r, int64_t n, const int32_t* __r
 // nwin * kSellWindow entries.
 __global__ void __launch_bounds__(kBuildThreads) k_sell_sort(int64_t n, int64_t nwin, const int32_t* __restrict__ rowptr, int32_t* __restrict__ perm)
 {
+  ::trl_detail::pdl_enter();
   __shared__ int bins[kBuildWarps][kSellKeys];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t win = static_cast<int64_t>(blockIdx.x) * kBuildWarps + w;
@@ -155,6 +156,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_sell_sort(int64_t n, int64_t 
 __global__ void __launch_bounds__(256) k_sell_slices(int64_t nslices, int C, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ perm,
                                                      int64_t* __restrict__ sptr, int64_t* __restrict__ part, unsigned long long* __restrict__ stats)
 {
+  ::trl_detail::pdl_enter();
   constexpr int PER = kScanItems / 256;
   __shared__ int64_t warp_tot[8];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -200,6 +202,7 @@ __global__ void __launch_bounds__(256) k_sell_slices(int64_t nslices, int C, con
 // stats[0]; sptr[0] = 0.
 __global__ void __launch_bounds__(1024) k_sell_scan_parts(int64_t nparts, int64_t* __restrict__ part, int64_t* __restrict__ sptr, unsigned long long* __restrict__ stats)
 {
+  ::trl_detail::pdl_enter();
   __shared__ int64_t warp_tot[32];
   __shared__ int64_t carry;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -231,6 +234,7 @@ __global__ void __launch_bounds__(1024) k_sell_scan_parts(int64_t nparts, int64_
 
 __global__ void __launch_bounds__(256) k_sell_add_parts(int64_t nslices, const int64_t* __restrict__ part, int64_t* __restrict__ sptr)
 {
+  ::trl_detail::pdl_enter();
   const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s < nslices) sptr[1 + s] += part[s / kScanItems];
 }
@@ -241,6 +245,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_sell_fill(int64_t nslices, in
                                                           const V* __restrict__ vals, const int32_t* __restrict__ perm, const int64_t* __restrict__ sptr,
                                                           int32_t* __restrict__ scol, V* __restrict__ sval)
 {
+  ::trl_detail::pdl_enter();
   const int lane = threadIdx.x & 31;
   const int64_t wstride = static_cast<int64_t>(gridDim.x) * kBuildWarps;
   const int q = lane % C, jj = lane / C, spj = 32 / C; // slots per warp step
@@ -303,6 +308,7 @@ __global__ void __launch_bounds__(kSpmmThreads, SellTune<T, BS, NBG, LONG>::MINB
     k_spmm_sell(int nslices, int nwin, int spw, int interleave, const int32_t* __restrict__ perm, const int64_t* __restrict__ sptr, const int32_t* __restrict__ scol,
                 const T* __restrict__ sval, const T* __restrict__ X, T* Y, T alpha, T beta, T gamma, const T* W, int nb, int64_t bstride)
 {
+  ::trl_detail::pdl_enter();
   using S = SellShape<T, BS>;
   constexpr int VEC = S::VEC, LPR = S::LPR, C = S::RPW, UG = SellTune<T, BS, NBG, LONG>::UG;
   const int lane = threadIdx.x & 31;
@@ -513,13 +519,13 @@ int trl_cuda_op_create(trl_cuda_handle h, const trl_csr* A, int bs, trl_cuda_op*
   if (!part) return fail(TRL_ENOMEM);
   auto* stats = reinterpret_cast<unsigned long long*>(part + nparts);
   cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), h->stream);
-  k_sell_sort<<<static_cast<unsigned>((op->nwin + kBuildWarps - 1) / kBuildWarps), kBuildThreads, 0, h->stream>>>(A->n, op->nwin, A->rowptr, op->perm);
+  launch(k_sell_sort, static_cast<unsigned>((op->nwin + kBuildWarps - 1) / kBuildWarps), kBuildThreads, 0, h->stream, A->n, op->nwin, A->rowptr, op->perm);
   if ((st = after_launch(h, "sell sort"))) return fail(st);
-  k_sell_slices<<<static_cast<unsigned>(nparts), 256, 0, h->stream>>>(op->nslices, C, A->rowptr, op->perm, op->sptr, part, stats);
+  launch(k_sell_slices, static_cast<unsigned>(nparts), 256, 0, h->stream, op->nslices, C, A->rowptr, op->perm, op->sptr, part, stats);
   if ((st = after_launch(h, "sell slices"))) return fail(st);
-  k_sell_scan_parts<<<1, 1024, 0, h->stream>>>(nparts, part, op->sptr, stats);
+  launch(k_sell_scan_parts, 1, 1024, 0, h->stream, nparts, part, op->sptr, stats);
   if ((st = after_launch(h, "sell scan"))) return fail(st);
-  k_sell_add_parts<<<static_cast<unsigned>((op->nslices + 255) / 256), 256, 0, h->stream>>>(op->nslices, part, op->sptr);
+  launch(k_sell_add_parts, static_cast<unsigned>((op->nslices + 255) / 256), 256, 0, h->stream, op->nslices, part, op->sptr);
   if ((st = after_launch(h, "sell scan"))) return fail(st);
   unsigned long long hs[2] = {0, 0};
   if ((st = trl_cuda_memcpy(h, hs, stats, sizeof hs, TRL_D2H))) return fail(st);
@@ -537,10 +543,10 @@ int trl_cuda_op_create(trl_cuda_handle h, const trl_csr* A, int bs, trl_cuda_op*
   if (op->stored > 0) {
     const unsigned grid = grid_for(h, op->nslices, kBuildWarps, 8);
     if (A->value_dtype == TRL_F64)
-      k_sell_fill<double><<<grid, kBuildThreads, 0, h->stream>>>(op->nslices, C, A->rowptr, A->colind, static_cast<const double*>(A->values), op->perm, op->sptr, op->scol,
+      launch(k_sell_fill<double>, grid, kBuildThreads, 0, h->stream, op->nslices, C, A->rowptr, A->colind, static_cast<const double*>(A->values), op->perm, op->sptr, op->scol,
                                                                   static_cast<double*>(op->sval));
     else
-      k_sell_fill<float><<<grid, kBuildThreads, 0, h->stream>>>(op->nslices, C, A->rowptr, A->colind, static_cast<const float*>(A->values), op->perm, op->sptr, op->scol,
+      launch(k_sell_fill<float>, grid, kBuildThreads, 0, h->stream, op->nslices, C, A->rowptr, A->colind, static_cast<const float*>(A->values), op->perm, op->sptr, op->scol,
                                                                  static_cast<float*>(op->sval));
     if ((st = after_launch(h, "sell fill"))) return fail(st);
   }
@@ -582,7 +588,7 @@ int trl_cuda_op_spmm(trl_cuda_handle h, trl_cuda_op op, const void* X, void* Y, 
   int st = TRL_OK;
   const int dtype = op->dtype;
   TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
-    const auto launch = [&](auto kernel, int minb) {
+    const auto run = [&](auto kernel, int minb) {
       static int resident[64]; // per device and instantiation of the kernel
       int& res = resident[h->device & 63];
       if (res == 0) {
@@ -591,13 +597,13 @@ int trl_cuda_op_spmm(trl_cuda_handle h, trl_cuda_op op, const void* X, void* Y, 
       }
       // one resident wave; every warp strides over the slices
       const unsigned grid = grid_for(h, op->nslices, kSpmmWarps, res);
-      kernel<<<grid, kSpmmThreads, 0, h->stream>>>(static_cast<int>(op->nslices), static_cast<int>(op->nwin), op->spw, op->interleave, op->perm, op->sptr, op->scol, static_cast<const T*>(op->sval),
+      trl_detail::launch(kernel, grid, kSpmmThreads, 0, h->stream, static_cast<int>(op->nslices), static_cast<int>(op->nwin), op->spw, op->interleave, op->perm, op->sptr, op->scol, static_cast<const T*>(op->sval),
                                                    static_cast<const T*>(X), static_cast<T*>(Y), static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma),
                                                    static_cast<const T*>(W), nb, op->n * BS);
     };
-    if (nb > 1) launch(k_spmm_sell<T, BS, 2, false>, SellTune<T, BS, 2, false>::MINB);
-    else if (op->long_rows) launch(k_spmm_sell<T, BS, 1, true>, SellTune<T, BS, 1, true>::MINB);
-    else launch(k_spmm_sell<T, BS, 1, false>, SellTune<T, BS, 1, false>::MINB);
+    if (nb > 1) run(k_spmm_sell<T, BS, 2, false>, SellTune<T, BS, 2, false>::MINB);
+    else if (op->long_rows) run(k_spmm_sell<T, BS, 1, true>, SellTune<T, BS, 1, true>::MINB);
+    else run(k_spmm_sell<T, BS, 1, false>, SellTune<T, BS, 1, false>::MINB);
     st = after_launch(h, "spmm (sliced ELL)");
   }));
   return st;

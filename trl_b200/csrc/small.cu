@@ -23,6 +23,7 @@ struct DiagValues {
 
 __global__ void k_mb_copy(double* __restrict__ dst, const double* __restrict__ src, int bs, int transpose)
 {
+  ::trl_detail::pdl_enter();
   const int e = threadIdx.x;
   if (e >= bs * bs) return;
   const int i = e / bs, j = e % bs;
@@ -31,6 +32,7 @@ __global__ void k_mb_copy(double* __restrict__ dst, const double* __restrict__ s
 
 __global__ void k_mb_mult(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C, int bs)
 {
+  ::trl_detail::pdl_enter();
   const int e = threadIdx.x;
   if (e >= bs * bs) return;
   const int i = e / bs, j = e % bs;
@@ -41,6 +43,7 @@ __global__ void k_mb_mult(const double* __restrict__ A, const double* __restrict
 
 __global__ void k_mb_set_diag(double* __restrict__ dst, DiagValues d, int bs)
 {
+  ::trl_detail::pdl_enter();
   const int i = threadIdx.x;
   if (i < bs) dst[i * bs + i] = d.v[i];
 }
@@ -48,6 +51,7 @@ __global__ void k_mb_set_diag(double* __restrict__ dst, DiagValues d, int bs)
 // max |T_ij| over the block matrix (one CTA) into *out
 __global__ void __launch_bounds__(1024) k_max_abs(const double* __restrict__ T, int64_t count, double* __restrict__ out)
 {
+  ::trl_detail::pdl_enter();
   __shared__ double red[32];
   double m = 0.0;
   for (int64_t e = threadIdx.x; e < count; e += blockDim.x) m = fmax(m, fabs(T[e]));
@@ -72,6 +76,7 @@ constexpr double kFlushRel = 1e-30;
 // dense column-major A (N x N) from the lower triangle of the block matrix T
 __global__ void k_assemble_dense(const double* __restrict__ T, int nblk, int bs, const double* __restrict__ tmax, double* __restrict__ A)
 {
+  ::trl_detail::pdl_enter();
   const int N = nblk * bs;
   const int64_t total = static_cast<int64_t>(N) * N;
   const double floor = kFlushRel * *tmax;
@@ -87,6 +92,7 @@ __global__ void k_assemble_dense(const double* __restrict__ T, int nblk, int bs,
 // rank of each eigenvalue in decreasing |theta| order (ties keep ascending index)
 __global__ void k_rank(const double* __restrict__ w, int N, int* __restrict__ perm, double* __restrict__ evals_sorted, const int* __restrict__ syevd_info, int* status)
 {
+  ::trl_detail::pdl_enter();
   if (blockIdx.x == 0 && threadIdx.x == 0 && *syevd_info != 0) atomicOr(status, TRL_DEV_EIGEN);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     const double ai = fabs(w[i]);
@@ -102,6 +108,7 @@ __global__ void k_rank(const double* __restrict__ w, int N, int* __restrict__ pe
 
 __global__ void k_scatter_evecs(const double* __restrict__ A, const int* __restrict__ perm, int nblk, int bs, double* __restrict__ Y)
 {
+  ::trl_detail::pdl_enter();
   const int N = nblk * bs;
   const int64_t total = static_cast<int64_t>(N) * N;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -119,6 +126,7 @@ __global__ void k_scatter_evecs(const double* __restrict__ A, const int* __restr
 __global__ void k_count_converged(const double* __restrict__ A, const int* __restrict__ perm, const double* __restrict__ evals_sorted, const double* __restrict__ beta, int nblk,
                                   int bs, int ncheck, double tol, int* __restrict__ count)
 {
+  ::trl_detail::pdl_enter();
   const int N = nblk * bs;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncheck; c += gridDim.x * blockDim.x) {
     const double* y = A + static_cast<int64_t>(perm[c]) * N + (nblk - 1) * bs;
@@ -172,7 +180,7 @@ int trl_cuda_mb_copy(trl_cuda_handle h, double* dst, const double* src, int bs, 
   if (dst == src && !transpose) return TRL_OK;
   if (dst == src) return set_error(h, TRL_EINVAL, "in-place transpose not supported");
   ProfScope prof(h, PROF_BLOCK_OPS, 16.0 * bs * bs);
-  k_mb_copy<<<1, bs * bs, 0, h->stream>>>(dst, src, bs, transpose);
+  launch(k_mb_copy, 1, bs * bs, 0, h->stream, dst, src, bs, transpose);
   return after_launch(h, "mb_copy");
 }
 
@@ -190,7 +198,7 @@ int trl_cuda_mb_mult(trl_cuda_handle h, const double* A, const double* B, double
   if (!valid_bs(bs) || !A || !B || !C) return set_error(h, TRL_EINVAL, "bad block mult arguments");
   if (C == A || C == B) return set_error(h, TRL_EINVAL, "block mult output must not alias an input");
   ProfScope prof(h, PROF_BLOCK_OPS, 24.0 * bs * bs, 2.0 * bs * bs * bs);
-  k_mb_mult<<<1, bs * bs, 0, h->stream>>>(A, B, C, bs);
+  launch(k_mb_mult, 1, bs * bs, 0, h->stream, A, B, C, bs);
   return after_launch(h, "mb_mult");
 }
 
@@ -201,7 +209,7 @@ int trl_cuda_mb_set_diagonal(trl_cuda_handle h, double* dst, const double* host_
   ProfScope prof(h, PROF_BLOCK_OPS, 8.0 * bs);
   DiagValues d{};
   for (int i = 0; i < bs; ++i) d.v[i] = host_values[i];
-  k_mb_set_diag<<<1, 32, 0, h->stream>>>(dst, d, bs);
+  launch(k_mb_set_diag, 1, 32, 0, h->stream, dst, d, bs);
   return after_launch(h, "mb_set_diagonal");
 }
 
@@ -256,19 +264,19 @@ int trl_cuda_small_eigen(trl_cuda_handle h, const double* T, int nblk, int bs, c
   }
 
   const unsigned g = grid_for(h, static_cast<int64_t>(N) * N, 256, 4);
-  k_max_abs<<<1, 1024, 0, h->stream>>>(T, static_cast<int64_t>(N) * N, tmax);
-  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, tmax, A);
+  launch(k_max_abs, 1, 1024, 0, h->stream, T, static_cast<int64_t>(N) * N, tmax);
+  launch(k_assemble_dense, g, 256, 0, h->stream, T, nblk, bs, tmax, A);
   if (int st = after_launch(h, "assemble")) return st;
   cs = cusolverDnDsyevd(sh, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, N, A, N, w, static_cast<double*>(h->syevd_work), lwork, info);
   if (cs != CUSOLVER_STATUS_SUCCESS) return set_error(h, TRL_ECUDA, "syevd failed (%d)", static_cast<int>(cs));
-  k_rank<<<(N + 255) / 256, 256, 0, h->stream>>>(w, N, perm, evals, info, h->d_status);
+  launch(k_rank, (N + 255) / 256, 256, 0, h->stream, w, N, perm, evals, info, h->d_status);
   if (int st = after_launch(h, "rank")) return st;
-  k_scatter_evecs<<<g, 256, 0, h->stream>>>(A, perm, nblk, bs, evecs);
+  launch(k_scatter_evecs, g, 256, 0, h->stream, A, perm, nblk, bs, evecs);
   if (int st = after_launch(h, "scatter")) return st;
   cudaMemsetAsync(count, 0, sizeof(int), h->stream);
   const int ncheck = nev < N ? nev : N;
   if (ncheck > 0) {
-    k_count_converged<<<(ncheck + 127) / 128, 128, 0, h->stream>>>(A, perm, evals, beta, nblk, bs, ncheck, tol, count);
+    launch(k_count_converged, (ncheck + 127) / 128, 128, 0, h->stream, A, perm, evals, beta, nblk, bs, ncheck, tol, count);
     if (int st = after_launch(h, "count")) return st;
   }
   char* pin = static_cast<char*>(pinned(h, w_bytes + 64));
@@ -395,6 +403,7 @@ template <int C, bool kGlobalRows>
 __global__ void __launch_bounds__(kTriThreads, 1)
     k_tridiag(double* __restrict__ A, int N, double* __restrict__ dout, double* __restrict__ eout, double* __restrict__ tau_out, double* __restrict__ refl)
 {
+  ::trl_detail::pdl_enter();
   namespace cg = cooperative_groups;
   constexpr int NW = kTriThreads / 32;
   constexpr int NP = C * NW; // partials per exchange
@@ -530,6 +539,7 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e2, in
 // w[i] = i-th smallest eigenvalue of the tridiagonal (d, e); one warp per eigenvalue
 __global__ void __launch_bounds__(256) k_bisect(const double* __restrict__ dg, const double* __restrict__ eg, int N, double* __restrict__ w)
 {
+  ::trl_detail::pdl_enter();
   __shared__ double d[kBisectMaxN], e2[kBisectMaxN];
   __shared__ double bounds[3];
   for (int j = threadIdx.x; j < N; j += blockDim.x) {
@@ -595,6 +605,7 @@ constexpr int kFactorRows = 5;
 __global__ void __launch_bounds__(32) k_tri_factor(const double* __restrict__ dg, const double* __restrict__ eg, int N, const double* __restrict__ w, const int* __restrict__ sel,
                                                    double* __restrict__ F, double* __restrict__ Z)
 {
+  ::trl_detail::pdl_enter();
   extern __shared__ __align__(16) double fs[]; // 5 x N
   const int t = blockIdx.x, lane = threadIdx.x;
   // ||T||_inf (Gershgorin) for the pivot floor
@@ -650,6 +661,7 @@ __global__ void __launch_bounds__(32) k_tri_factor(const double* __restrict__ dg
 // z_t <- (T - lambda_t I)^{-1} z_t, scaled to unit max-norm
 __global__ void __launch_bounds__(32) k_tri_solve(int N, const double* __restrict__ F, double* __restrict__ Z)
 {
+  ::trl_detail::pdl_enter();
   extern __shared__ __align__(16) double fs[]; // 5 x N factors, N vector
   const int t = blockIdx.x, lane = threadIdx.x;
   for (int idx = lane; idx < kFactorRows * N; idx += 32) fs[idx] = F[static_cast<size_t>(t) * kFactorRows * N + idx];
@@ -705,6 +717,7 @@ __global__ void __launch_bounds__(32) k_tri_solve(int N, const double* __restric
 template <bool kGlobal>
 __global__ void __launch_bounds__(kTriThreads) k_tri_gs(int N, int K, double* __restrict__ Z)
 {
+  ::trl_detail::pdl_enter();
   extern __shared__ __align__(16) double zsm[]; // K x N
   double* const zs = kGlobal ? Z : zsm;
   __shared__ double coef[kTriMaxVec];
@@ -752,6 +765,7 @@ constexpr int kWyVecs = 1; // vectors per CTA: the chunk products are latency-bo
 // T of chunk c (reflectors c * kWyRows ...) into Tw[c][kWyRows][kWyRows]
 __global__ void __launch_bounds__(256) k_wy_factor(const double* __restrict__ refl, const double* __restrict__ tau, int N, double* __restrict__ Tw)
 {
+  ::trl_detail::pdl_enter();
   extern __shared__ __align__(16) double vs[]; // kWyRows x N
   __shared__ double G[kWyRows][kWyRows], Tt[kWyRows][kWyRows];
   const int R = N - 2;
@@ -798,6 +812,7 @@ __global__ void __launch_bounds__(256) k_wy_factor(const double* __restrict__ re
 __global__ void __launch_bounds__(256) k_backtransform(const double* __restrict__ Z, int K, int N, const double* __restrict__ refl, const double* __restrict__ Tw,
                                                        double* __restrict__ X)
 {
+  ::trl_detail::pdl_enter();
   extern __shared__ __align__(16) double sm[]; // kWyRows x N reflectors | kWyVecs x N vectors
   double* vs = sm;
   double* xs = sm + kWyRows * N;
@@ -853,6 +868,7 @@ __global__ void __launch_bounds__(256) k_backtransform(const double* __restrict_
 // selected ascending indices: sel[t] (ascending), slot[c] = t for rank c < K
 __global__ void k_select(const int* __restrict__ perm, int K, int* __restrict__ sel, int* __restrict__ slot)
 {
+  ::trl_detail::pdl_enter();
   const int c = threadIdx.x;
   if (c >= K) return;
   const int a = perm[c];
@@ -865,6 +881,7 @@ __global__ void k_select(const int* __restrict__ perm, int K, int* __restrict__ 
 // Y in block layout: column c < K is X[slot[c]], the rest zero
 __global__ void k_scatter_partial(const double* __restrict__ X, const int* __restrict__ slot, int nblk, int bs, int K, double* __restrict__ Y)
 {
+  ::trl_detail::pdl_enter();
   const int N = nblk * bs;
   const int64_t total = static_cast<int64_t>(N) * N;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -881,6 +898,7 @@ __global__ void k_scatter_partial(const double* __restrict__ X, const int* __res
 __global__ void k_count_partial(const double* __restrict__ X, const int* __restrict__ slot, const double* __restrict__ evals_sorted, const double* __restrict__ beta, int nblk, int bs,
                                 int ncheck, double tol, int* __restrict__ count)
 {
+  ::trl_detail::pdl_enter();
   const int N = nblk * bs;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncheck; c += gridDim.x * blockDim.x) {
     const double* y = X + static_cast<int64_t>(slot[c]) * N + (nblk - 1) * bs;
@@ -898,6 +916,7 @@ __global__ void k_count_partial(const double* __restrict__ X, const int* __restr
 // zero the block-layout columns >= K of Y
 __global__ void k_zero_cols(double* __restrict__ Y, int nblk, int bs, int K)
 {
+  ::trl_detail::pdl_enter();
   const int N = nblk * bs;
   const int64_t total = static_cast<int64_t>(N) * N;
   for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -985,7 +1004,7 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   const TriVariant* tv = tri_variant(h->device, N);
   if (N < 3 || kvec > kTriMaxVec || !tv) {
     if (int st = trl_cuda_small_eigen(h, T, nblk, bs, beta, nev, tol, evals, evecs, host_evals, host_nconv)) return st;
-    k_zero_cols<<<grid_for(h, static_cast<int64_t>(N) * N, 256, 4), 256, 0, h->stream>>>(evecs, nblk, bs, kvec);
+    launch(k_zero_cols, grid_for(h, static_cast<int64_t>(N) * N, 256, 4), 256, 0, h->stream, evecs, nblk, bs, kvec);
     return after_launch(h, "zero columns");
   }
   ProfScope prof(h, PROF_SMALL_EIGEN, 16.0 * N * N);
@@ -1015,8 +1034,8 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
   double* tmax = reinterpret_cast<double*>(ws + (sizeof(double) * doubles + sizeof(int) * ints + 15) / 16 * 16);
 
   const unsigned g = grid_for(h, static_cast<int64_t>(N) * N, 256, 4);
-  k_max_abs<<<1, 1024, 0, h->stream>>>(T, static_cast<int64_t>(N) * N, tmax);
-  k_assemble_dense<<<g, 256, 0, h->stream>>>(T, nblk, bs, tmax, A);
+  launch(k_max_abs, 1, 1024, 0, h->stream, T, static_cast<int64_t>(N) * N, tmax);
+  launch(k_assemble_dense, g, 256, 0, h->stream, T, nblk, bs, tmax, A);
   if (int st = after_launch(h, "assemble")) return st;
   cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream);
   {
@@ -1026,31 +1045,31 @@ extern "C" int trl_cuda_small_eigen_partial(trl_cuda_handle h, const double* T, 
     cudaLaunchKernelEx(&cfg, tv->fn, A, N, d, e, tau, refl);
     if (int st = after_launch(h, "tridiagonalise")) return st;
   }
-  k_bisect<<<(N + 7) / 8, 256, 0, h->stream>>>(d, e, N, w);
+  launch(k_bisect, (N + 7) / 8, 256, 0, h->stream, d, e, N, w);
   if (int st = after_launch(h, "bisect")) return st;
-  k_rank<<<(N + 255) / 256, 256, 0, h->stream>>>(w, N, perm, evals, flags, h->d_status);
+  launch(k_rank, (N + 255) / 256, 256, 0, h->stream, w, N, perm, evals, flags, h->d_status);
   if (int st = after_launch(h, "rank")) return st;
-  k_select<<<1, kTriMaxVec, 0, h->stream>>>(perm, K, sel, slot);
+  launch(k_select, 1, kTriMaxVec, 0, h->stream, perm, K, sel, slot);
   if (int st = after_launch(h, "select")) return st;
-  k_tri_factor<<<K, 32, sizeof(double) * kFactorRows * N, h->stream>>>(d, e, N, w, sel, F, Z);
+  launch(k_tri_factor, K, 32, sizeof(double) * kFactorRows * N, h->stream, d, e, N, w, sel, F, Z);
   if (int st = after_launch(h, "tridiagonal factor")) return st;
   for (int it = 0; it < kTriIters; ++it) {
-    k_tri_solve<<<K, 32, sizeof(double) * (kFactorRows + 1) * N, h->stream>>>(N, F, Z);
+    launch(k_tri_solve, K, 32, sizeof(double) * (kFactorRows + 1) * N, h->stream, N, F, Z);
     if (int st = after_launch(h, "inverse iteration")) return st;
   }
-  if (sizeof(double) * NK > kTriGsMaxBytes) k_tri_gs<true><<<1, kTriThreads, 0, h->stream>>>(N, K, Z);
-  else k_tri_gs<false><<<1, kTriThreads, sizeof(double) * NK, h->stream>>>(N, K, Z);
+  if (sizeof(double) * NK > kTriGsMaxBytes) launch(k_tri_gs<true>, 1, kTriThreads, 0, h->stream, N, K, Z);
+  else launch(k_tri_gs<false>, 1, kTriThreads, sizeof(double) * NK, h->stream, N, K, Z);
   if (int st = after_launch(h, "gram-schmidt")) return st;
   const int nch = (N - 2 + kWyRows - 1) / kWyRows;
-  k_wy_factor<<<nch, 256, sizeof(double) * kWyRows * N, h->stream>>>(refl, tau, N, Tw);
+  launch(k_wy_factor, nch, 256, sizeof(double) * kWyRows * N, h->stream, refl, tau, N, Tw);
   if (int st = after_launch(h, "wy factor")) return st;
-  k_backtransform<<<(K + kWyVecs - 1) / kWyVecs, 256, sizeof(double) * (kWyRows + kWyVecs) * N, h->stream>>>(Z, K, N, refl, Tw, X);
+  launch(k_backtransform, (K + kWyVecs - 1) / kWyVecs, 256, sizeof(double) * (kWyRows + kWyVecs) * N, h->stream, Z, K, N, refl, Tw, X);
   if (int st = after_launch(h, "back-transform")) return st;
-  k_scatter_partial<<<g, 256, 0, h->stream>>>(X, slot, nblk, bs, kvec, evecs);
+  launch(k_scatter_partial, g, 256, 0, h->stream, X, slot, nblk, bs, kvec, evecs);
   if (int st = after_launch(h, "scatter")) return st;
   const int ncheck = nev < kvec ? nev : kvec;
   if (ncheck > 0) {
-    k_count_partial<<<(ncheck + 127) / 128, 128, 0, h->stream>>>(X, slot, evals, beta, nblk, bs, ncheck, tol, flags + 1);
+    launch(k_count_partial, (ncheck + 127) / 128, 128, 0, h->stream, X, slot, evals, beta, nblk, bs, ncheck, tol, flags + 1);
     if (int st = after_launch(h, "count")) return st;
   }
   const size_t w_bytes = sizeof(double) * N;

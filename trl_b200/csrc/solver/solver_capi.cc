@@ -161,7 +161,7 @@ PhaseOut run_phase_r(const std::shared_ptr<Context>& ctx, const trl_csr* A, cons
 // plus the kept blocks' gathers and stores.
 
 struct RefineOut {
-  bool applicable = false; // false: the kept Ritz values straddle zero (use the Lanczos refinement)
+  bool applicable = false; // false: the Lanczos refinement takes over (the filter does not apply, or is predicted or found slower)
   bool converged = false;
   unsigned rounds = 0;
   unsigned degree = 0;   // total filter degree (FP32 and FP64 rounds)
@@ -204,15 +204,23 @@ public:
   /// the last Rayleigh-Ritz step, |theta| descending. lanczos_estimate_s > 0: before the
   /// first filter round the refinement compares its own predicted time with this estimate of
   /// the Lanczos refinement's and gives up (applicable = false, X the Rayleigh-Ritz vectors)
-  /// when the filter would take longer.
+  /// when the filter would take longer; it also gives up at the start of a later round once
+  /// it has run three times that estimate.
   RefineOut run(double* X, double lanczos_estimate_s = 0.0)
   {
+    const auto t_run = std::chrono::steady_clock::now(); // every round starts after a synchronising Rayleigh-Ritz step
+    const auto seconds_since = [](std::chrono::steady_clock::time_point t) { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count(); };
     RefineOut out;
     double lo = 0.0, hi = 0.0;
     ctx_->check(trl_cuda_csr_gershgorin(h_, A_, p_.alpha, p_.beta, &lo, &hi), "refine bounds");
     double* cur = X;
     double* spare = static_cast<double*>(Y_.get());
-    orthonormalize(cur);
+    {
+      EventTimer t(static_cast<cudaStream_t>(trl_cuda_stream(h_)));
+      t.start();
+      orthonormalize(cur);
+      t_orth_ = t.stop(); // the cost of one re-orthonormalisation inside the filter
+    }
     const unsigned N = kr_ * bs;
     bool use32 = op32_ != nullptr;
     double prev_res = 0.0; // residual at the start of the last FP32 round
@@ -252,11 +260,21 @@ public:
         // predicted filter time: the degrees to reach the tolerance at the predicted rate
         // (optimistic early on, so this errs towards the filter) times one degree, measured
         // as the Rayleigh-Ritz step's multi-block SpMM (each degree is one such SpMM plus a
-        // share of re-orthonormalisation and Rayleigh-Ritz steps, counted as 25% more)
+        // share of re-orthonormalisation and Rayleigh-Ritz steps, counted as 25% more).
+        // The two-sided filter is held to a 4x margin: on an indefinite spectrum the
+        // interval [-b, b] leaves unwanted eigenvalues close to both of its ends, and its
+        // early rate estimate was up to 25x too high (Zipf pattern, 4.2M rows, block size 4:
+        // predicted 6.3 s, took 160 s), against about 5x for a one-sided filter.
+        // A degree also carries its share of the re-orthonormalisations, one per chunk of
+        // degrees (the FP64 chunk length below).
         const double degrees = std::log(std::max(res / p_.tol, 1.0)) / rw;
-        out.predicted_s = 1.25 * degrees * t_spmm_;
+        const double chunk64 = rt - rw > 0.0 ? std::clamp(std::log(1e6) / (rt - rw), 4.0, static_cast<double>(kMaxDegree)) : static_cast<double>(kMaxDegree);
+        out.predicted_s = (one_sided ? 1.25 : 5.0) * degrees * (t_spmm_ + t_orth_ / chunk64);
         if (out.predicted_s > lanczos_estimate_s) return finish(out, cur, X); // not applicable: the Lanczos refinement is cheaper
       }
+      // a filter that has already taken three times the Lanczos refinement's estimate gives
+      // way to it, from the current Rayleigh-Ritz vectors
+      if (round > 0 && lanczos_estimate_s > 0.0 && seconds_since(t_run) > 3.0 * lanczos_estimate_s) return finish(out, cur, X);
       // FP32 rounds while the residual is above what FP32 vectors resolve and FP32 rounds
       // still make progress (a round that gains less than 1.05x has met the FP32 floor)
       if (use32 && prev_res > 0.0 && !(res < prev_res / 1.05)) use32 = false;
@@ -329,6 +347,7 @@ private:
   const trl_csr* A_;
   std::shared_ptr<const SellOp> op64_, op32_;
   double t_spmm_ = 0.0; // seconds of one multi-block SpMM over the kept blocks
+  double t_orth_ = 0.0; // seconds of one orthonormalisation of the kept blocks
   trl_solve_params p_;
   unsigned kr_;
   std::int64_t n_;
@@ -529,6 +548,10 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
         stage("refinement done");
         info->refine_predicted_s = r.predicted_s;
         info->refine_lanczos_estimate_s = lanczos_s;
+        // the filter's work, also when it handed over to the Lanczos refinement
+        info->refine_rounds = r.rounds;
+        info->refine_degree = r.degree;
+        info->refine_degree_fp32 = r.degree32;
         if (r.applicable) {
           info->refine_used = TRL_REFINE_CHEBYSHEV;
           refined = true;
@@ -536,9 +559,6 @@ int solve_device(const std::shared_ptr<Context>& ctx, const trl_solve_params& p,
           out.restarts = 0;
           out.applies = 0;
           out.evals = r.evals;
-          info->refine_rounds = r.rounds;
-          info->refine_degree = r.degree;
-          info->refine_degree_fp32 = r.degree32;
         }
       }
       if (!refined) {

@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
                                                                          const T* __restrict__ vals, const T* __restrict__ X, T* Y, T alpha, T beta, T gamma,
                                                                          const T* W, int nb, int64_t bstride)
 {
+  ::trl_detail::pdl_enter();
   using S = SpmmShape<T, BS>;
   constexpr int VEC = S::VEC, LPR = S::LPR, RPW = S::RPW, UG = S::UG, CH = S::CH, PF = S::PF;
   constexpr int WPC = kThreads / 32;
@@ -224,6 +225,7 @@ __global__ void __launch_bounds__(kThreads, SpmmShape<T, BS>::MINB) k_spmm(int64
 __global__ void __launch_bounds__(kThreads) k_sddmm(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const double* __restrict__ X, int k,
                                                     const double* __restrict__ w, double* __restrict__ out)
 {
+  ::trl_detail::pdl_enter();
   const int lane = threadIdx.x & 31;
   const int64_t warp_global = static_cast<int64_t>(blockIdx.x) * (kThreads / 32) + (threadIdx.x >> 5);
   const int64_t warp_stride = static_cast<int64_t>(gridDim.x) * (kThreads / 32);
@@ -270,18 +272,18 @@ static int spmm_impl(trl_cuda_context* h, const trl_csr* A, int dtype, const voi
   TRL_DISPATCH_DT(dtype, TRL_DISPATCH_BS(bs, {
     using S = SpmmShape<T, BS>;
     // one resident wave: every warp strides over the rows (its rowptr prefetch pays off)
-    const auto launch = [&](auto kernel) {
+    const auto run = [&](auto kernel) {
       static int resident = 0; // one per instantiation of the kernel
       if (resident == 0) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreads, 0) != cudaSuccess || resident < 1) resident = S::MINB;
         cudaGetLastError();
       }
       const unsigned grid = grid_for(h, (A->n + S::RPW - 1) / S::RPW, kThreads / 32, resident);
-      kernel<<<grid, kThreads, 0, h->stream>>>(A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
+      trl_detail::launch(kernel, grid, kThreads, 0, h->stream, A->n, A->rowptr, A->colind, static_cast<const T*>(A->values), static_cast<const T*>(X), static_cast<T*>(Y),
                                                static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma), static_cast<const T*>(W), nb, A->n * BS);
     };
-    if (nb > 1) launch(k_spmm<T, BS, true>);
-    else launch(k_spmm<T, BS, false>);
+    if (nb > 1) run(k_spmm<T, BS, true>);
+    else run(k_spmm<T, BS, false>);
     st = after_launch(h, "spmm");
   }));
   return st;
@@ -313,7 +315,7 @@ int trl_cuda_sddmm(trl_cuda_handle h, const trl_csr* P, const double* X, int k, 
   if (P->n == 0 || P->nnz == 0) return TRL_OK;
   ProfScope prof(h, PROF_SDDMM, 12.0 * P->nnz + 4.0 * (P->n + 1) + 8.0 * P->n * k, 3.0 * P->nnz * k);
   const unsigned grid = grid_for(h, P->n, kThreads / 32, 16);
-  k_sddmm<<<grid, kThreads, 0, h->stream>>>(P->n, P->rowptr, P->colind, X, k, w, out);
+  launch(k_sddmm, grid, kThreads, 0, h->stream, P->n, P->rowptr, P->colind, X, k, w, out);
   return after_launch(h, "sddmm");
 }
 
@@ -365,6 +367,7 @@ namespace {
 __global__ void __launch_bounds__(256) k_norm1(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const void* __restrict__ vals, int f64,
                                                double alpha, double beta, unsigned long long* __restrict__ out)
 {
+  ::trl_detail::pdl_enter();
   double best = 0.0;
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     double s = 0.0;
@@ -398,6 +401,7 @@ __device__ __forceinline__ unsigned long long ordered_bits(double x)
 __global__ void __launch_bounds__(256) k_gershgorin(int64_t n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind, const void* __restrict__ vals,
                                                     int f64, double alpha, double beta, unsigned long long* __restrict__ lo_hi)
 {
+  ::trl_detail::pdl_enter();
   double lo = INFINITY, hi = -INFINITY;
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n; r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     double c = beta, rad = 0.0;
@@ -431,7 +435,7 @@ extern "C" int trl_cuda_csr_gershgorin(trl_cuda_handle h, const trl_csr* A, doub
   if (!d) return TRL_ENOMEM;
   const unsigned long long init[2] = {~0ull, 0ull};
   if (int st = trl_cuda_memcpy(h, d, init, sizeof init, TRL_H2D)) return st;
-  k_gershgorin<<<grid_for(h, A->n, 256, 8), 256, 0, h->stream>>>(A->n, A->rowptr, A->colind, A->values, A->value_dtype == TRL_F64, alpha, beta, d);
+  launch(k_gershgorin, grid_for(h, A->n, 256, 8), 256, 0, h->stream, A->n, A->rowptr, A->colind, A->values, A->value_dtype == TRL_F64, alpha, beta, d);
   if (int st = after_launch(h, "csr_gershgorin")) return st;
   unsigned long long bits[2] = {0, 0};
   if (int st = trl_cuda_memcpy(h, bits, d, sizeof bits, TRL_D2H)) return st;
@@ -451,7 +455,7 @@ extern "C" int trl_cuda_csr_norm1(trl_cuda_handle h, const trl_csr* A, double al
   unsigned long long* d = static_cast<unsigned long long*>(workspace(h, 64));
   if (!d) return TRL_ENOMEM;
   cudaMemsetAsync(d, 0, sizeof(unsigned long long), h->stream);
-  k_norm1<<<grid_for(h, A->n, 256, 8), 256, 0, h->stream>>>(A->n, A->rowptr, A->colind, A->values, A->value_dtype == TRL_F64, alpha, beta, d);
+  launch(k_norm1, grid_for(h, A->n, 256, 8), 256, 0, h->stream, A->n, A->rowptr, A->colind, A->values, A->value_dtype == TRL_F64, alpha, beta, d);
   if (int st = after_launch(h, "csr_norm1")) return st;
   unsigned long long bits = 0;
   if (int st = trl_cuda_memcpy(h, &bits, d, sizeof bits, TRL_D2H)) return st;
