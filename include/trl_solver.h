@@ -42,8 +42,7 @@ enum trl_reorth { TRL_REORTH_MGS = 0, TRL_REORTH_CGS2 = 1, TRL_REORTH_CGS_IFNEED
  * predicted rate x one measured multi-block SpMM and a share of one measured
  * re-orthonormalisation; a two-sided filter, for kept values on both sides of zero, with a
  * 4x margin) and hands over to the Lanczos refinement when that is predicted cheaper
- * (estimated from the FP32 phase's time and the orders of magnitude left), or later, at the
- * start of a round, once the filter has taken three times that estimate. */
+ * (estimated from the FP32 phase's time and the orders of magnitude left). */
 enum trl_refine { TRL_REFINE_LANCZOS = 0, TRL_REFINE_CHEBYSHEV = 1, TRL_REFINE_AUTO = 2 };
 
 typedef struct trl_solve_params {
@@ -88,8 +87,8 @@ typedef struct trl_solve_info {
   double op_norm1;          /* ||op||_1 = max row sum of |alpha*A + beta*I| */
   unsigned long long kernel_launches; /* kernels launched by the backend during the call */
   double h2d_bytes, d2h_bytes;        /* host<->device traffic of the call */
-  unsigned refine_rounds;   /* Chebyshev refinement: Rayleigh-Ritz rounds (0: not run; also
-                               counted when it handed over to the Lanczos refinement) */
+  unsigned refine_rounds;   /* Chebyshev refinement: Rayleigh-Ritz rounds (0: not run; 1 with
+                               refine_used = TRL_REFINE_LANCZOS: handed over after its first) */
   unsigned refine_degree;   /* Chebyshev refinement: total filter degree */
   unsigned refine_degree_fp32; /* Chebyshev refinement: of which applied in FP32 */
   int refine_used;              /* TRL_MODE_MIXED: the refinement that ran (trl_refine) */

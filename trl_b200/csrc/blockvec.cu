@@ -335,27 +335,38 @@ __device__ __forceinline__ double slice_sum(const double* __restrict__ partial, 
   return ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
 }
 
-// out[e] = sum_c partial[c][e]: 32 outputs per CTA, 32 slices of the chunk range per output
-// (one warp each, slice_sum); the slices are combined in a fixed order, so the result does
-// not depend on scheduling.
+// out[e] = sum_c partial[c][e]: OPC outputs per CTA, SL = 1024 / OPC slices of the chunk
+// range per output (slice_sum); the slices are combined in a fixed order, so the result
+// does not depend on scheduling. OPC = 32 for long outputs (one warp per slice, coalesced);
+// OPC = 8 for short ones (the b x b blocks of one or a few basis blocks): eight times the
+// CTAs and a quarter of the loads per thread, so that ~600 partials take one memory round.
 constexpr int kRedThreads = 1024;
+template <int OPC>
 __global__ void __launch_bounds__(kRedThreads) k_reduce_partials(const double* __restrict__ partial, int chunks, int64_t len, double* __restrict__ out,
-                                                                 const int* __restrict__ cond = nullptr)
+                                                                 const int* __restrict__ cond)
 {
   ::trl_detail::pdl_enter();
   if (cond && *cond == 0) return;
-  constexpr int SL = kRedThreads / 32;
-  __shared__ double part[SL][33];
-  const int o = threadIdx.x & 31, s = threadIdx.x >> 5;
-  const int64_t e = static_cast<int64_t>(blockIdx.x) * 32 + o;
+  constexpr int SL = kRedThreads / OPC;
+  __shared__ double part[SL][OPC + 1];
+  const int o = threadIdx.x % OPC, s = threadIdx.x / OPC;
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * OPC + o;
   part[s][o] = e < len ? slice_sum<SL>(partial, chunks, len, e, s) : 0.0;
   __syncthreads();
   if (s == 0 && e < len) {
     double t = 0.0;
-#pragma unroll
+#pragma unroll 8
     for (int q = 0; q < SL; ++q) t += part[q][o];
     out[e] = t;
   }
+}
+
+// Launches the fixed-order reduction of `chunks` partial rows of `len` doubles into out.
+inline cudaError_t launch_reduce(cudaStream_t stream, const double* partial, int64_t chunks, int64_t len, double* out, const int* cond)
+{
+  if (len <= 1024 && chunks > 128)
+    return ::trl_detail::launch(k_reduce_partials<8>, static_cast<unsigned>((len + 7) / 8), kRedThreads, 0, stream, partial, static_cast<int>(chunks), len, out, cond);
+  return ::trl_detail::launch(k_reduce_partials<32>, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, stream, partial, static_cast<int>(chunks), len, out, cond);
 }
 
 // ---------------------------------------------------------------- block GEMM
@@ -766,36 +777,51 @@ __global__ void k_select_block(const int* __restrict__ flag, const double* __res
   if (e < count) dst[e] = *flag ? a[e] : b[e];
 }
 
-// ---------------------------------------------------------------- small Cholesky, one CTA
+// ---------------------------------------------------------------- small Cholesky
 // Gram matrix G from `chunks` partial sums (chunks = 0: G given), then G = L L^T reading
 // the lower triangle, Uinv = L^{-T} for the apply, and R <- L^T (first pass) or
 // R <- L^T R (so that X_in = X_out R across passes). All in shared memory; the factor and
 // the inverse are column-parallel over one warp. A pivot <= 0 (or NaN) records
 // TRL_DEV_CHOLESKY and writes Uinv = I, leaving the apply a no-op.
+// With partial sums the reduction is spread over ceil(BS^2 / kFactorOPC) CTAs, each
+// summing kFactorOPC entries of G in a fixed order into gsum; the CTA that finishes last
+// (a ticket counter, left at zero again) factors. Every entry is summed by one CTA in one
+// order, so the result does not depend on scheduling.
+constexpr int kFactorOPC = 8;
 template <int BS>
 __global__ void __launch_bounds__(kRedThreads) k_gram_factor(const double* __restrict__ src, int chunks, double* __restrict__ Uinv, double* __restrict__ R, int first,
-                                                             int* status)
+                                                             int* status, double* gsum, unsigned* ticket)
 {
   ::trl_detail::pdl_enter();
-  constexpr int SL = kRedThreads / 32; // slices of the chunk range per output
+  constexpr int OPC = kFactorOPC;
+  constexpr int SL = kRedThreads / OPC; // slices of the chunk range per entry
   __shared__ double G[BS * BS], L[BS][BS + 1], Li[BS][BS + 1], Ro[BS * BS];
-  __shared__ double part[SL][33];
-  __shared__ int bad;
+  __shared__ double part[SL][OPC + 1];
+  __shared__ int bad, last;
   const int tid = threadIdx.x;
-  // 1. G (the same fixed-order reduction as k_reduce_partials)
+  // 1. G (the same fixed-order reduction as k_reduce_partials<8>)
   if (chunks > 0) {
-    for (int e0 = 0; e0 < BS * BS; e0 += 32) {
-      const int o = tid & 31, s = tid >> 5, e = e0 + o;
-      part[s][o] = e < BS * BS ? slice_sum<SL>(src, chunks, BS * BS, e, s) : 0.0;
-      __syncthreads();
-      if (s == 0 && e < BS * BS) {
-        double t = 0.0;
-#pragma unroll
-        for (int q = 0; q < SL; ++q) t += part[q][o];
-        G[e] = t;
-      }
-      __syncthreads();
+    const int o = tid % OPC, s = tid / OPC, e = static_cast<int>(blockIdx.x) * OPC + o;
+    part[s][o] = e < BS * BS ? slice_sum<SL>(src, chunks, BS * BS, e, s) : 0.0;
+    __syncthreads();
+    if (s == 0 && e < BS * BS) {
+      double t = 0.0;
+#pragma unroll 8
+      for (int q = 0; q < SL; ++q) t += part[q][o];
+      gsum[e] = t;
     }
+    if (gridDim.x > 1) {
+      __threadfence(); // this CTA's entries of gsum are visible before its ticket is taken
+      __syncthreads();
+      if (tid == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+      __syncthreads();
+      if (!last) return;
+      __threadfence();
+      if (tid == 0) *ticket = 0u;
+    }
+    else
+      __syncthreads();
+    for (int e = tid; e < BS * BS; e += blockDim.x) G[e] = __ldcg(gsum + e); // L2: written by other CTAs
   }
   else {
     for (int e = tid; e < BS * BS; e += blockDim.x) G[e] = src[e];
@@ -888,7 +914,7 @@ int launch_block_dot_jc(trl_cuda_context* h, const T* V, int nblk, const T* W, i
   launch(k_block_dot<T, BS, JC, G>, grid, kThreads, 0, h->stream, V, n * BS, nblk, W, n, rows_per_cta, partial, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream, partial, static_cast<int>(chunks), len, C, cond);
+  launch_reduce(h->stream, partial, chunks, len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -913,7 +939,7 @@ int launch_block_dot_two(trl_cuda_context* h, const T* A, const T* B, const T* W
   launch(k_block_dot<T, BS, JC, G>, dim3(1, static_cast<unsigned>(chunks)), kThreads, 0, h->stream, A, vstride, 2, W, n, rows_per_cta, partial, nullptr);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream, partial, static_cast<int>(chunks), len, C, nullptr);
+  launch_reduce(h->stream, partial, chunks, len, C, nullptr);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -946,7 +972,7 @@ int launch_block_dot_bulk(trl_cuda_context* h, const T* V, int nblk, const T* W,
   launch(k_block_dot_bulk<T, BS, JC, S, TB>, dim3(gj, static_cast<unsigned>(chunks)), kThreads, smem, h->stream, V, n * BS, nblk, W, n, rows_per_cta, partial, h->d_status, cond);
   int st = after_launch(h, "block_dot");
   if (st) return st;
-  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, h->stream, partial, static_cast<int>(chunks), len, C, cond);
+  launch_reduce(h->stream, partial, chunks, len, C, cond);
   return after_launch(h, "block_dot reduce");
 }
 
@@ -1016,7 +1042,7 @@ int launch_update_gram(trl_cuda_context* h, const T* in, int MB, const double* c
   int chunks = 0;
   int st = launch_update_gram_partials<T, BS>(h, in, MB, coef, out, n, accumulate, sign, cond, &partial, &chunks);
   if (st) return st;
-  launch(k_reduce_partials, (BS * BS + 31) / 32, kRedThreads, 0, h->stream, partial, chunks, BS * BS, G, cond);
+  launch_reduce(h->stream, partial, chunks, BS * BS, G, cond);
   return after_launch(h, "update_gram reduce");
 }
 
@@ -1284,12 +1310,15 @@ int trl_cuda_cholqr_gram(trl_cuda_handle h, int dtype, void* X, int64_t n, int b
   double* small = static_cast<double*>(small_scratch(h));
   if (!small) return TRL_ENOMEM;
   double* Uinv = small + 256;
+  double* gsum = small + 512;                                // the factor's reduced Gram entries
+  unsigned* ticket = reinterpret_cast<unsigned*>(small + 768); // zero between launches
   ProfScope prof(h, PROF_CHOLQR, 2.0 * passes * n * bs * elt_size(dtype), 4.0 * passes * n * bs * bs);
   const double* src = G0; // the Gram matrix, or per-CTA partial sums of it
   int chunks = 0;
   for (int p = 0; p < passes; ++p) {
     int st = TRL_OK;
-    TRL_DISPATCH_BS(bs, launch(k_gram_factor<BS>, 1, kRedThreads, 0, h->stream, src, chunks, Uinv, R, p == 0, h->d_status));
+    TRL_DISPATCH_BS(bs, launch(k_gram_factor<BS>, chunks > 0 ? static_cast<unsigned>((BS * BS + kFactorOPC - 1) / kFactorOPC) : 1u, kRedThreads, 0, h->stream, src, chunks,
+                               Uinv, R, p == 0, h->d_status, gsum, ticket));
     st = after_launch(h, "cholqr factor");
     if (st) return st;
     if (p + 1 < passes) {
@@ -1522,7 +1551,7 @@ static int noalloc_dot(cudaStream_t stream, int sms, double* partial, const T* V
   // so nothing left in the array by an earlier call is used and nothing needs clearing
   launch(k_block_dot<T, BS, JC, G>, dim3(gj, static_cast<unsigned>(chunks)), kThreads, 0, stream, V, n * BS, nblk, W, n, rows_per_cta, partial, nullptr);
   if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
-  launch(k_reduce_partials, static_cast<unsigned>((len + 31) / 32), kRedThreads, 0, stream, partial, static_cast<int>(chunks), len, C, nullptr);
+  launch_reduce(stream, partial, chunks, len, C, nullptr);
   if (cudaGetLastError() != cudaSuccess) return TRL_ECUDA;
   return TRL_OK;
 }

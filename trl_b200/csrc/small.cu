@@ -156,6 +156,8 @@ void* small_scratch(trl_cuda_context* h)
       set_error(h, TRL_ENOMEM, "scratch allocation failed");
       return nullptr;
     }
+    // zeroed once: the CholQR factor's ticket counter (doubles 768..) must start at zero
+    cudaMemsetAsync(h->d_small, 0, 1024 * sizeof(double), h->stream);
   }
   return h->d_small;
 }
