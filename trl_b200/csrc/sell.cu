@@ -272,9 +272,9 @@ constexpr int kSpmmThreads = 256;
 constexpr int kSpmmWarps = kSpmmThreads / 32;
 
 // Per instantiation: NBG blocks accumulated per pass over a slice (1 for the single-block
-// SpMM; the multi-block SpMM takes two blocks per pass and re-reads a slice's indices and
-// values, from L2, for each pair), UG slots per group, and the CTAs per SM the registers
-// must allow.
+// SpMM; the multi-block SpMM takes up to kSellBlocksPerPass blocks per pass and re-reads a
+// slice's indices and values, from L2, for each further pass), UG slots per group, and the
+// CTAs per SM the registers must allow.
 template <typename T, int BS, int NBG, bool LONG>
 struct SellTune {
   static constexpr int lane_bytes = SellShape<T, BS>::VEC * static_cast<int>(sizeof(T));
@@ -283,10 +283,18 @@ struct SellTune {
   // gathers in flight per lane at two CTAs per SM; short rows prefer more warps with fewer
   // slots each (measured on B200: 96^3 stencil, 7 slots per slice, 0.56 of the copy peak
   // with 2 slots x 4 CTAs against 0.53 with 8 x 2; elasticity, 81 slots, 0.50 with 8 x 2
-  // against 0.39 with 2 x 4)
-  static constexpr int UG = NBG == 1 ? (LONG ? 8 : (ug > 4 ? 4 : ug)) : 2;
+  // against 0.39 with 2 x 4). Several blocks per pass keep one slot per lane in flight for
+  // each block.
+  static constexpr int UG = NBG == 1 ? (LONG ? 8 : (ug > 4 ? 4 : ug)) : (NBG > 2 ? 1 : 2);
   static constexpr int MINB = NBG == 1 ? (LONG ? 2 : 4) : 2;
 };
+
+// Blocks per pass of the multi-block SpMM (the Chebyshev filter's kept blocks). Measured on
+// B200 with 6 blocks of the 96^3 stencil, bs 8, behind an L2 flush (fraction of the copy
+// peak, FP64 / FP32): 2 blocks x 2 slots per pass 0.40 / 0.40; 3 x 2: 0.49 / 0.47; 3 x 1 at 3
+// CTAs per SM: 0.40 / 0.39; 4 x 1: 0.40 / 0.31; 6 x 1 (one pass, 128 registers, 2 CTAs per
+// SM): 0.55 / 0.50.
+constexpr int kSellBlocksPerPass = 6;
 
 // Asks L2 to fetch [p, p + bytes) (a bulk prefetch: no registers, no shared memory). p and
 // bytes are multiples of 16.
@@ -601,7 +609,7 @@ int trl_cuda_op_spmm(trl_cuda_handle h, trl_cuda_op op, const void* X, void* Y, 
                                                    static_cast<const T*>(X), static_cast<T*>(Y), static_cast<T>(alpha), static_cast<T>(beta), static_cast<T>(gamma),
                                                    static_cast<const T*>(W), nb, op->n * BS);
     };
-    if (nb > 1) run(k_spmm_sell<T, BS, 2, false>, SellTune<T, BS, 2, false>::MINB);
+    if (nb > 1) run(k_spmm_sell<T, BS, kSellBlocksPerPass, false>, SellTune<T, BS, kSellBlocksPerPass, false>::MINB);
     else if (op->long_rows) run(k_spmm_sell<T, BS, 1, true>, SellTune<T, BS, 1, true>::MINB);
     else run(k_spmm_sell<T, BS, 1, false>, SellTune<T, BS, 1, false>::MINB);
     st = after_launch(h, "spmm (sliced ELL)");
