@@ -7,6 +7,8 @@
   temporary's write is deferred, and written exactly when a later operation needs it.
 * The C-ABI libraries load without a GPU and export every function include/*.h declares.
 * The multi-rank reduction bench.py uses (max over ranks) on a 2-rank gloo group.
+* The launch discipline of trl_b200/csrc: every kernel starts with the programmatic-
+  dependent-launch wait, and every launch goes through the library's launch helper.
 """
 import ctypes
 import os
@@ -158,3 +160,38 @@ def test_solve_csr_host_rejects_bad_eigenvector_buffers():
     for bad in (np.zeros((A.n, 9)), np.zeros((A.n, 10), dtype=np.float32), np.zeros((10, A.n)).T, ro, [[0.0] * 10] * A.n):
         with pytest.raises(ValueError):
             native.solve_csr_host(A, X0, evecs_out=bad, bs=4, nev=10, ncv=160)
+
+
+def _csrc_files():
+    d = os.path.join(ROOT, "trl_b200", "csrc")
+    return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith(".cu")]
+
+
+def _strip_comments(src: str) -> str:
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return re.sub(r"//[^\n]*", "", src)
+
+
+def test_every_kernel_waits_for_its_predecessor_first():
+    """Kernels are launched with programmatic stream serialization (trl_detail::launch), so a
+    kernel may be scheduled while the previous one of its stream still runs. Each must
+    begin with pdl_enter() (griddepcontrol.wait) before it touches global memory; this
+    checks that the first statement of every __global__ function is that call."""
+    kernels = 0
+    for path in _csrc_files():
+        src = _strip_comments(open(path).read())
+        for m in re.finditer(r"__global__", src):
+            body = src.index("{", m.end())
+            first = src[body + 1:].lstrip()
+            name = re.search(r"(k_\w+)\s*\(", src[m.end():body]).group(1)
+            assert first.startswith("::trl_detail::pdl_enter();"), f"{os.path.basename(path)}: {name} does not start with pdl_enter()"
+            kernels += 1
+    assert kernels >= 40
+
+
+def test_every_launch_goes_through_the_launch_helper():
+    """No kernel is launched with <<<>>> (which would bypass the launch attributes the
+    library sets); the cluster launch of the tridiagonalisation uses cudaLaunchKernelEx."""
+    for path in _csrc_files():
+        src = _strip_comments(open(path).read())
+        assert "<<<" not in src, os.path.basename(path)
