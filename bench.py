@@ -172,7 +172,7 @@ def cpu_info() -> dict:
 
 
 def load_reference_counts() -> dict:
-    with open(os.path.join(ROOT, "tests", "golden", "cfg2_reference.json")) as f:
+    with open(os.path.join(ROOT, "tests", "golden", "aniso96_reference.json")) as f:
         return json.load(f)
 
 
@@ -237,7 +237,7 @@ def reference_arm(args, world, rank):
                          "sample": f"reference BlockLanczos (ModifiedGS, CholQR) on the headline workload: one run of {len(cyc)} restart cycles; "
                                    f"each step is one steady-state cycle (cycles {2 + args.warmup}..{len(cyc)}, mean {est['cycle_mean_s']:.3f} s, "
                                    f"sd {est['cycle_stdev_s']:.3f} s); full solve projected as cycle 1 + {ref['restarts'] - 1} x mean "
-                                   f"({ref['restarts']} restarts: the reference's own count for this workload, tests/golden/cfg2_reference.json)"},
+                                   f"({ref['restarts']} restarts: the reference's own count for this workload, tests/golden/aniso96_reference.json)"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

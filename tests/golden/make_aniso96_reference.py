@@ -1,10 +1,10 @@
 """Runs the oracle (the reference's OpenMP BlockLanczos, default ModifiedGS, single-pass
 CholQR) to convergence on the 96^3 anisotropic Laplacian with axis coefficients (1, 10, 100):
 bs 8, nev 32, ncv 384, tol 1e-10, start block problems.initial_block(n, 8, seed=42).
-Writes tests/golden/cfg2_reference.json: restart and operator-apply counts, wall time and
+Writes tests/golden/aniso96_reference.json: restart and operator-apply counts, wall time and
 thread count of this host, and the 32 eigenvalues.
 
-    OMP_NUM_THREADS=8 python tests/golden/make_cfg2_reference.py
+    OMP_NUM_THREADS=8 python tests/golden/make_aniso96_reference.py
 """
 import json
 import os
@@ -47,7 +47,7 @@ def main():
         "evals": r["evals"][:32].tolist(),
         "max_rel_err_vs_analytic": float(np.max(np.abs(r["evals"][:32] - exact) / exact)),
     }
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cfg2_reference.json")
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "aniso96_reference.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     print(json.dumps({k: v for k, v in out.items() if k != "evals"}))

@@ -96,7 +96,7 @@ def test_small_dense_order_and_count(oracle):
     assert nconv == 8
 
 
-def test_oracle_solves_cfg1_to_analytic(oracle):
+def test_oracle_solves_laplace128_to_analytic(oracle):
     A = P.laplace2d(128)
     X0 = P.initial_block(A.n, 4, seed=42)
     r = oracle.solve_csr(A, 4, 10, 160, X0, tol=1e-8)

@@ -65,7 +65,7 @@ def max_principal_sine(Xa, Xb, evals):
 
 
 @pytest.fixture(scope="module")
-def cfg1_oracle(oracle):
+def laplace128_oracle(oracle):
     A = P.laplace2d(128)
     X0 = P.initial_block(A.n, 4, seed=42)
     r = oracle.solve_csr(A, 4, 10, 160, X0, tol=1e-8, ritz=True)
@@ -75,8 +75,8 @@ def cfg1_oracle(oracle):
 
 @pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS2, native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS, native.TRL_REORTH_PARTIAL])
 @pytest.mark.parametrize("passes", [1, 2])
-def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
-    A, X0, ref = cfg1_oracle
+def test_laplace128_fp64_matches_oracle(laplace128_oracle, reorth, passes):
+    A, X0, ref = laplace128_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8, reorth=reorth, cholqr_passes=passes)
     assert out["converged"]
     exact = P.laplace2d_eigenvalues(128)[:10]
@@ -91,10 +91,10 @@ def test_cfg1_fp64_matches_oracle(cfg1_oracle, reorth, passes):
 
 
 @pytest.mark.parametrize("pairs", [0, 1])
-def test_partial_reorthogonalisation_with_and_without_pairs(cfg1_oracle, pairs):
+def test_partial_reorthogonalisation_with_and_without_pairs(laplace128_oracle, pairs):
     """partial_pairs = 1 (default) also projects the step after each fired sketch test; both
     settings give the reference's eigenpairs with orthonormal Ritz vectors."""
-    A, X0, ref = cfg1_oracle
+    A, X0, ref = laplace128_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8, reorth=native.TRL_REORTH_PARTIAL, partial_pairs=pairs)
     assert out["converged"]
     assert np.max(np.abs(out["evals"] - ref["evals"][:10]) / np.abs(ref["evals"][:10])) < 1e-10
@@ -104,12 +104,12 @@ def test_partial_reorthogonalisation_with_and_without_pairs(cfg1_oracle, pairs):
     assert abs(out["restarts"] - ref["iterations"]) <= max(3, ref["iterations"] // 5)
 
 
-def test_eigenvectors_into_the_callers_buffer(cfg1_oracle):
+def test_eigenvectors_into_the_callers_buffer(laplace128_oracle):
     """evecs_out (here page-locked, as a repeated caller keeps it) receives exactly what the
     allocating call returns, and is returned itself."""
     import torch
 
-    A, X0, ref = cfg1_oracle
+    A, X0, ref = laplace128_oracle
     kw = dict(bs=4, nev=10, ncv=160, tol=1e-8)
     buf = torch.full((A.n, 10), float("nan"), dtype=torch.float64).pin_memory().numpy()
     mine = native.solve_csr_host(A, X0, evecs_out=buf, **kw)
@@ -120,11 +120,11 @@ def test_eigenvectors_into_the_callers_buffer(cfg1_oracle):
 
 
 @pytest.mark.parametrize("reorth", [native.TRL_REORTH_CGS_IFNEEDED, native.TRL_REORTH_MGS])
-def test_fused_and_call_by_call_execution_agree(cfg1_oracle, reorth):
+def test_fused_and_call_by_call_execution_agree(laplace128_oracle, reorth):
     """batching = 1 fuses the three-term step's product/subtract pairs (deferring the
     temporary) and the restart rotation; batching = 0 issues every driver call as its own
     kernel. Both must give the reference's eigenpairs."""
-    A, X0, ref = cfg1_oracle
+    A, X0, ref = laplace128_oracle
     outs = [native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-8, reorth=reorth, batching=b) for b in (0, 1)]
     for out in outs:
         assert out["converged"]
@@ -136,8 +136,8 @@ def test_fused_and_call_by_call_execution_agree(cfg1_oracle, reorth):
         assert outs[1]["kernel_launches"] < outs[0]["kernel_launches"]
 
 
-def test_cfg1_mixed_reaches_fp64_accuracy(cfg1_oracle):
-    A, X0, ref = cfg1_oracle
+def test_laplace128_mixed_reaches_fp64_accuracy(laplace128_oracle):
+    A, X0, ref = laplace128_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-5)
     assert out["converged"]
     exact = P.laplace2d_eigenvalues(128)[:10]
@@ -147,11 +147,11 @@ def test_cfg1_mixed_reaches_fp64_accuracy(cfg1_oracle):
 
 
 @pytest.mark.parametrize("refine,refine_fp32", [(native.TRL_REFINE_CHEBYSHEV, 1), (native.TRL_REFINE_CHEBYSHEV, 0), (native.TRL_REFINE_LANCZOS, 1)])
-def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine, refine_fp32):
+def test_mixed_refinements_reach_fp64_accuracy(laplace128_oracle, refine, refine_fp32):
     """Both FP64 refinements of the mixed mode from the FP32 phase's kept Ritz vectors: the
     Chebyshev-filtered subspace iteration with Rayleigh-Ritz (with and without its FP32
     filter rounds), and a BlockLanczos restart."""
-    A, X0, ref = cfg1_oracle
+    A, X0, ref = laplace128_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-4, refine=refine,
                                 refine_fp32=refine_fp32)
     assert out["converged"]
@@ -169,11 +169,11 @@ def test_mixed_refinements_reach_fp64_accuracy(cfg1_oracle, refine, refine_fp32)
 
 
 @pytest.mark.parametrize("mode", [native.TRL_MODE_FP64, native.TRL_MODE_MIXED])
-def test_partial_and_full_projected_eigensolvers_agree(cfg1_oracle, mode):
+def test_partial_and_full_projected_eigensolvers_agree(laplace128_oracle, mode):
     """The restart's projected eigenproblem solved for the kept eigenvectors only (cluster
     tridiagonalisation + inverse iteration, the default) and for all of them (cuSOLVER
     syevd): same eigenpairs, same number of restarts."""
-    A, X0, ref = cfg1_oracle
+    A, X0, ref = laplace128_oracle
     kw = dict(bs=4, nev=10, ncv=160, tol=1e-10, mode=mode, fp32_tol=1e-4)
     part = native.solve_csr_host(A, X0, small_eigen_full=0, **kw)
     full = native.solve_csr_host(A, X0, small_eigen_full=1, **kw)
@@ -185,10 +185,10 @@ def test_partial_and_full_projected_eigensolvers_agree(cfg1_oracle, mode):
 
 
 @pytest.mark.parametrize("fp32_ncv", [0, 96])
-def test_mixed_loose_fp32_phase_filters_in_fp32(cfg1_oracle, fp32_ncv):
+def test_mixed_loose_fp32_phase_filters_in_fp32(laplace128_oracle, fp32_ncv):
     """A loose FP32 phase (fp32_tol 1e-2, optionally on a smaller FP32 basis) leaves most of
     the work to the filter: its FP32 rounds run first and the FP64 rounds finish at 1e-10."""
-    A, X0, ref = cfg1_oracle
+    A, X0, ref = laplace128_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_tol=1e-2, fp32_ncv=fp32_ncv)
     assert out["converged"]
     assert 0 < out["refine_degree_fp32"] < out["refine_degree"]
@@ -198,8 +198,8 @@ def test_mixed_loose_fp32_phase_filters_in_fp32(cfg1_oracle, fp32_ncv):
     assert max_principal_sine(out["evecs"], ref["ritz"], out["evals"]) < 1e-5
 
 
-def test_fp32_ncv_must_be_a_multiple_of_the_block_size(cfg1_oracle):
-    A, X0, _ = cfg1_oracle
+def test_fp32_ncv_must_be_a_multiple_of_the_block_size(laplace128_oracle):
+    A, X0, _ = laplace128_oracle
     with pytest.raises(native.TrlError):
         native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-10, mode=native.TRL_MODE_MIXED, fp32_ncv=98)
 
@@ -225,16 +225,16 @@ def test_mixed_with_kept_values_on_both_sides_of_zero(oracle, refine):
     assert out["max_theta_residual"] < 1e-10
 
 
-def test_fp32_mode_accuracy_is_stated(cfg1_oracle):
-    A, X0, ref = cfg1_oracle
+def test_fp32_mode_accuracy_is_stated(laplace128_oracle):
+    A, X0, ref = laplace128_oracle
     out = native.solve_csr_host(A, X0, bs=4, nev=10, ncv=160, tol=1e-5, mode=native.TRL_MODE_FP32)
     assert out["converged"]
     exact = P.laplace2d_eigenvalues(128)[:10]
     assert np.max(np.abs(out["evals"] - exact) / exact) < 1e-5
 
 
-def test_device_entry_point_matches_host_entry_point(cfg1_oracle):
-    A, X0, ref = cfg1_oracle
+def test_device_entry_point_matches_host_entry_point(laplace128_oracle):
+    A, X0, ref = laplace128_oracle
     h = native.Handle(0)
     A64 = native.DeviceCSRTensors.from_host(A)
     X0d = torch.from_numpy(X0).cuda()
@@ -321,14 +321,14 @@ def test_invalid_parameters_raise():
 
 
 @pytest.mark.slow
-def test_cfg2_fp64_and_mixed_to_analytic():
+def test_aniso96_fp64_and_mixed_to_analytic():
     """The 96^3 anisotropic Laplacian (1,10,100): 32 largest to 1e-10, both modes, against the
     analytic spectrum and against the eigenvalues and restart count of the reference's own
-    OpenMP BlockLanczos on the same matrix and start block (tests/golden/cfg2_reference.json,
-    written by tests/golden/make_cfg2_reference.py)."""
+    OpenMP BlockLanczos on the same matrix and start block (tests/golden/aniso96_reference.json,
+    written by tests/golden/make_aniso96_reference.py)."""
     A = P.anisotropic3d(96)
     exact = P.anisotropic3d_eigenvalues(96, k=32)
-    with open(GOLDEN / "cfg2_reference.json") as f:
+    with open(GOLDEN / "aniso96_reference.json") as f:
         ref = json.load(f)
     ref_evals = np.asarray(ref["evals"])
     X0 = P.initial_block(A.n, 8, seed=42)
