@@ -8,8 +8,9 @@ largest eigenpairs, basis 48 blocks (ncv = 384), thick restart, tolerance 1e-10;
 synthetic start block. A "step" is one complete solve (Ritz vectors and true residuals
 included) from the same start block with the operator resident in HBM.
 
-The same JSON line carries the other workloads of the benchmark configurations, each solved
-once in FP64 and once in mixed precision after a short warm-up solve (`workloads`):
+On one GPU the same JSON line carries the other workloads of the benchmark configurations,
+each solved once in FP64 and once in mixed precision after a short warm-up solve
+(`workloads`; not repeated by the replicas of a multi-GPU run):
   elast64  3 dofs per node on a 64^3 node grid, 27-point coupling (n = 786,432, 61.7M
            entries), the 64 smallest eigenpairs through sigma*I - A, block size 8;
   diff512  generalised K x = lambda M x on a 512^2 grid (log-normal edge conductivities,
@@ -521,8 +522,10 @@ def trl_arm(args, world, rank, local):
 
     # ---- the other workloads of the benchmark configurations ----
     wl = {}
-    names = [w for w in args.workloads.split(",") if w and w != "aniso96"]
-    for name in names:  # every rank solves (replicas); rank 0 reports
+    # single-GPU runs only: replicas on more GPUs would repeat the same per-GPU solves (and
+    # each rank would generate the 145M-entry Zipf pattern on the host)
+    names = [w for w in args.workloads.split(",") if w and w != "aniso96"] if world == 1 else []
+    for name in names:
         t0 = time.time()
         wl[name] = secondary(h, name, args.secondary_modes.split(","))
         for row in wl[name]:
