@@ -195,3 +195,17 @@ def test_every_launch_goes_through_the_launch_helper():
     for path in _csrc_files():
         src = _strip_comments(open(path).read())
         assert "<<<" not in src, os.path.basename(path)
+
+
+def test_integration_example_compiles():
+    """The documented C++ usage (tests/host/integration_example.cc) compiles against the
+    reference's headers and this repository's include/."""
+    from oracle import oracle as O
+
+    ref_inc = os.path.join(O.reference_root(), "include")
+    if not os.path.isdir(os.path.join(ref_inc, "trl")):
+        pytest.skip("the reference headers are not present")
+    src = os.path.join(ROOT, "tests", "host", "integration_example.cc")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    r = subprocess.run(["/usr/bin/g++", "-std=c++20", "-fsyntax-only", f"-I{ref_inc}", f"-I{ROOT}/include", f"-I{cuda_inc}", src], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
